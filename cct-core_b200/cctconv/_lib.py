@@ -1,0 +1,158 @@
+"""ctypes binding of libcctconv.so (the C-ABI declared in include/cct_conv.h).
+
+The library is built in-tree (``cct-core_b200/csrc/libcctconv.so``).  There is
+no fallback: if the shared library is missing or fails to load, importing
+this module raises.
+"""
+import ctypes
+import os
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = Path(os.environ.get("CCT_CONV_LIB", _PKG.parent / "csrc" / "libcctconv.so"))
+
+# status codes
+OK, EINVAL, ENOTSUP, ENOMEM, ECUDA, ETIMEOUT, ENODEV = 0, -1, -2, -3, -4, -5, -6
+# policies (numeric values are the ABI's)
+BORDER_ZERO, BORDER_CLAMP, BORDER_CYCLIC, BORDER_VALID, BORDER_FULL = range(5)
+CROSS_CORRELATION, CONVOLUTION = 0, 1
+SAMPLE_NONE, SAMPLE_DOWN, SAMPLE_UP = 0, 1, 2
+(PLANE_BY_PLANE, PROJECT_FRAME, PROJECT_FRAME_BLOCK_REDUCE_SUM, BACK_PROJECT_FRAME,
+ BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM) = range(5)
+PREC_FP32, PREC_BF16X3 = 0, 1
+ALGO_AUTO, ALGO_DIRECT, ALGO_FFT = 0, 1, 2
+FLAG_RELU = 0x1
+PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT = 0, 1, 2, 3
+
+
+class ConvDesc(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32),
+        ("image_rows", ctypes.c_int32),
+        ("image_cols", ctypes.c_int32),
+        ("image_planes", ctypes.c_int32),
+        ("filter_rows", ctypes.c_int32),
+        ("filter_cols", ctypes.c_int32),
+        ("filter_planes", ctypes.c_int32),
+        ("batch_size", ctypes.c_int32),
+        ("border", ctypes.c_int32),
+        ("orientation", ctypes.c_int32),
+        ("sampling", ctypes.c_int32),
+        ("step", ctypes.c_int32),
+        ("vector_mode", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("algo", ctypes.c_int32),
+        ("flags", ctypes.c_uint32),
+    ]
+
+    def key(self):
+        return tuple(getattr(self, n) for n, _ in self._fields_)
+
+
+class CctError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+# Every symbol include/cct_conv.h declares, with (restype, argtypes).
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+_PI32 = ctypes.POINTER(ctypes.c_int32)
+SIGNATURES = {
+    "cct_conv_desc_init": (None, [ctypes.POINTER(ConvDesc)]),
+    "cct_conv_output_shape": (_I, [ctypes.POINTER(ConvDesc), _PI32, _PI32, _PI32]),
+    "cct_conv_plan_create": (_I, [ctypes.POINTER(ConvDesc), ctypes.POINTER(_P)]),
+    "cct_conv_plan_destroy": (_I, [_P]),
+    "cct_conv_plan_algo": (_I, [_P, _PI32]),
+    "cct_conv_plan_set_static_filter": (_I, [_P, _P]),
+    "cct_conv_run": (_I, [_P, _P, _P, _P, _P]),
+    "cct_conv_run_host": (_I, [_P, _P, _P, _P, _P]),
+    "cct_conv_separable": (_I, [_I32, _I32, _I32, _P, _P, _I32, _P, _I32, _I32, _I32, _P, _P, _P]),
+    "cct_malloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
+    "cct_free": (_I, [_P]),
+    "cct_memcpy_h2d": (_I, [_P, _P, ctypes.c_size_t, _P]),
+    "cct_memcpy_d2h": (_I, [_P, _P, ctypes.c_size_t, _P]),
+    "cct_stream_create": (_I, [ctypes.POINTER(_P)]),
+    "cct_stream_destroy": (_I, [_P]),
+    "cct_stream_synchronize": (_I, [_P]),
+    "cct_last_error_string": (ctypes.c_char_p, []),
+    "cct_abi_version": (_I, []),
+    "cct_launch_count": (ctypes.c_uint64, []),
+}
+
+
+def _load():
+    if not LIB_PATH.exists():
+        raise ImportError(f"libcctconv.so not built: {LIB_PATH} (run `make -C cct-core_b200/csrc`)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def check(status):
+    if status != OK:
+        raise CctError(status, LIB.cct_last_error_string().decode(errors="replace"))
+    return status
+
+
+def new_desc(**fields):
+    d = ConvDesc()
+    LIB.cct_conv_desc_init(ctypes.byref(d))
+    for k, v in fields.items():
+        setattr(d, k, int(v))
+    return d
+
+
+def output_shape(desc):
+    r, c, p = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    check(LIB.cct_conv_output_shape(ctypes.byref(desc), ctypes.byref(r), ctypes.byref(c),
+                                    ctypes.byref(p)))
+    return r.value, c.value, p.value
+
+
+class Plan:
+    """Owning wrapper of a cct_conv_plan."""
+
+    def __init__(self, desc):
+        self.desc = desc
+        self.shape = output_shape(desc)
+        h = ctypes.c_void_p()
+        check(LIB.cct_conv_plan_create(ctypes.byref(desc), ctypes.byref(h)))
+        self.handle = h
+        a = ctypes.c_int32()
+        check(LIB.cct_conv_plan_algo(h, ctypes.byref(a)))
+        self.algo = a.value
+
+    def set_static_filter(self, host_ptr):
+        check(LIB.cct_conv_plan_set_static_filter(self.handle, ctypes.c_void_p(host_ptr)))
+
+    def run(self, x_ptr, f_ptr, y_ptr, stream=0):
+        check(LIB.cct_conv_run(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(f_ptr),
+                               ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream)))
+
+    def run_host(self, x_ptr, f_ptr, y_ptr, stream=0):
+        check(LIB.cct_conv_run_host(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(f_ptr),
+                                    ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self.handle:
+            LIB.cct_conv_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def launch_count():
+    return int(LIB.cct_launch_count())

@@ -1,0 +1,345 @@
+// C-ABI of libcctconv: descriptor validation, plans, dispatch, memory helpers.
+//
+// The descriptor rules restate ConvolveHyperKernel.outputFieldType
+// (hyperkernels/ConvolveHyperKernel.scala:1297-1450) and the legality checks of
+// DynamicConvolutionGenerator.convolveDirectly
+// (generator/DynamicConvolutionGenerator.scala:484-539).
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "cct_internal.h"
+
+namespace cct {
+
+static thread_local char g_err[512] = "no error";
+static std::atomic<uint64_t> g_launches{0};
+
+int set_error(int status, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return status;
+}
+
+int check_cuda(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return CCT_OK;
+  const int status = e == cudaErrorMemoryAllocation ? CCT_ENOMEM : CCT_ECUDA;
+  return set_error(status, "%s: %s", what, cudaGetErrorString(e));
+}
+
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Resolve and validate a descriptor.  Returns CCT_OK or CCT_EINVAL with the
+// reference's error text.
+static int resolve(const cct_conv_desc *d, ConvGeom *g) {
+  if (!d) return set_error(CCT_EINVAL, "null descriptor");
+  if (d->struct_size != (int32_t)sizeof(cct_conv_desc))
+    return set_error(CCT_EINVAL, "descriptor struct_size %d != %d", d->struct_size,
+                     (int)sizeof(cct_conv_desc));
+  if (d->image_rows < 1 || d->image_cols < 1 || d->filter_rows < 1 || d->filter_cols < 1)
+    return set_error(CCT_EINVAL, "field and filter sizes must be positive");
+  if (d->image_planes < 0 || d->filter_planes < 0)
+    return set_error(CCT_EINVAL, "plane counts must be >= 0");
+  if (d->border < CCT_BORDER_ZERO || d->border > CCT_BORDER_FULL)
+    return set_error(CCT_EINVAL, "bad border policy %d", d->border);
+  if (d->orientation != CCT_CROSS_CORRELATION && d->orientation != CCT_CONVOLUTION)
+    return set_error(CCT_EINVAL, "bad filter orientation %d", d->orientation);
+  if (d->vector_mode < CCT_PLANE_BY_PLANE || d->vector_mode > CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+    return set_error(CCT_EINVAL, "bad vector mode %d", d->vector_mode);
+  if (d->precision != CCT_PREC_FP32 && d->precision != CCT_PREC_BF16X3)
+    return set_error(CCT_EINVAL, "bad precision %d", d->precision);
+  if (d->algo < CCT_ALGO_AUTO || d->algo > CCT_ALGO_FFT)
+    return set_error(CCT_EINVAL, "bad algorithm %d", d->algo);
+  if (d->flags & ~CCT_FLAG_RELU) return set_error(CCT_EINVAL, "unknown flags 0x%x", d->flags);
+
+  int sampling = d->sampling;
+  if (sampling < CCT_SAMPLE_NONE || sampling > CCT_SAMPLE_UP)
+    return set_error(CCT_EINVAL, "bad sampling policy %d", sampling);
+  if (sampling != CCT_SAMPLE_NONE && d->step < 1)
+    return set_error(CCT_EINVAL, "sampling step must be >= 1");
+  // CogFunctionAPI.scala:1139-1143: Upsample(1) / Downsample(1) are NoSampling.
+  if (sampling != CCT_SAMPLE_NONE && d->step == 1) sampling = CCT_SAMPLE_NONE;
+  const int step = sampling == CCT_SAMPLE_NONE ? 1 : d->step;
+
+  const int R = d->filter_rows, S = d->filter_cols;
+  if (d->border != CCT_BORDER_VALID && d->border != CCT_BORDER_FULL && (R % 2 == 0 || S % 2 == 0))
+    return set_error(CCT_EINVAL, "filter must be of odd shape for border policy %d", d->border);
+  if (sampling == CCT_SAMPLE_DOWN) {
+    int cr = 0, cc = 0;
+    if (d->border == CCT_BORDER_VALID) { cr = R - 1; cc = S - 1; }
+    if (d->border == CCT_BORDER_FULL) { cr = 1 - R; cc = 1 - S; }
+    if ((d->image_rows - cr) % step != 0 || (d->image_cols - cc) % step != 0)
+      return set_error(CCT_EINVAL,
+                       "The size of the input for convolution must be divisible by the "
+                       "downsampling step size after border contraction.");
+  }
+  if (sampling == CCT_SAMPLE_UP && d->border == CCT_BORDER_CLAMP)
+    return set_error(CCT_EINVAL, "Integrated upsampling with BorderClamp convolution not supported");
+
+  long long ur = d->image_rows, uc = d->image_cols;
+  if (sampling == CCT_SAMPLE_UP) { ur *= step; uc *= step; }
+  long long orow = ur, ocol = uc;
+  if (d->border == CCT_BORDER_VALID) { orow = ur - R + 1; ocol = uc - S + 1; }
+  if (d->border == CCT_BORDER_FULL) { orow = ur + R - 1; ocol = uc + S - 1; }
+  if (orow < 1 || ocol < 1) return set_error(CCT_EINVAL, "BorderValid filter larger than the input");
+  if (sampling == CCT_SAMPLE_DOWN) { orow = (orow + step - 1) / step; ocol = (ocol + step - 1) / step; }
+  if (orow > (1 << 30) || ocol > (1 << 30)) return set_error(CCT_EINVAL, "output too large");
+
+  const int pin = d->image_planes < 1 ? 1 : d->image_planes;
+  const int pf = d->filter_planes < 1 ? 1 : d->filter_planes;
+  const int batch = d->batch_size < 1 ? 1 : d->batch_size;
+  int pout, n = 1, groups = 1, terms = 1;
+  if (d->vector_mode == CCT_PLANE_BY_PLANE) {
+    if (!(d->image_planes == 0 || d->filter_planes == 0 || d->image_planes == d->filter_planes))
+      return set_error(CCT_EINVAL,
+                       "plane-by-plane convolution needs a ScalarField operand or equal tensor shapes");
+    pout = d->image_planes == 0 ? pf : pin;
+  } else {
+    if (pin % batch != 0)
+      return set_error(CCT_EINVAL, "Input tensorshape points %d must be a multiple of the batchSize %d",
+                       pin, batch);
+    n = pin / batch;
+    if (pf % n != 0)
+      return set_error(CCT_EINVAL, "filter tensor length %d not a multiple of per-image tensor length %d",
+                       pf, n);
+    groups = pf / n;
+    if (d->vector_mode == CCT_PROJECT_FRAME || d->vector_mode == CCT_BACK_PROJECT_FRAME) {
+      pout = pf * batch;
+    } else {
+      pout = batch * groups;
+      terms = n;
+    }
+  }
+
+  g->H = d->image_rows;
+  g->W = d->image_cols;
+  g->OH = (int)orow;
+  g->OW = (int)ocol;
+  g->R = R;
+  g->S = S;
+  g->low_r = d->border == CCT_BORDER_FULL ? R - 1 : (d->border == CCT_BORDER_VALID ? 0 : (R - 1) / 2);
+  g->low_c = d->border == CCT_BORDER_FULL ? S - 1 : (d->border == CCT_BORDER_VALID ? 0 : (S - 1) / 2);
+  g->border = d->border;
+  g->orient = d->orientation;
+  g->down = sampling == CCT_SAMPLE_DOWN ? step : 1;
+  g->up = sampling == CCT_SAMPLE_UP ? step : 1;
+  g->mode = d->vector_mode;
+  g->pin = pin;
+  g->pf = pf;
+  g->pout = pout;
+  g->batch = batch;
+  g->n = n;
+  g->groups = groups;
+  g->terms = terms;
+  g->flags = d->flags;
+  return CCT_OK;
+}
+
+}  // namespace cct
+
+using namespace cct;
+
+enum { ALGO_DIRECT = 0, ALGO_FRAME_F32 = 1, ALGO_FRAME_BF16X3 = 2, ALGO_FFT = 3 };
+
+struct cct_conv_plan {
+  cct_conv_desc desc;
+  ConvGeom g;
+  int algo;
+  int device;
+  size_t x_elems, f_elems, y_elems;
+  float *static_filter;  // device copy of a static filter, or null
+  // run_host staging (allocated on the first cct_conv_run_host call)
+  float *d_x, *d_f, *d_y;
+};
+
+extern "C" {
+
+void cct_conv_desc_init(cct_conv_desc *d) {
+  if (!d) return;
+  memset(d, 0, sizeof(*d));
+  d->struct_size = (int32_t)sizeof(cct_conv_desc);
+  d->image_rows = d->image_cols = 1;
+  d->filter_rows = d->filter_cols = 1;
+  d->batch_size = 1;
+  d->border = CCT_BORDER_ZERO;
+  d->orientation = CCT_CONVOLUTION;
+  d->sampling = CCT_SAMPLE_NONE;
+  d->step = 1;
+  d->vector_mode = CCT_PLANE_BY_PLANE;
+  d->precision = CCT_PREC_FP32;
+  d->algo = CCT_ALGO_AUTO;
+}
+
+int cct_conv_output_shape(const cct_conv_desc *d, int32_t *rows, int32_t *cols, int32_t *planes) {
+  ConvGeom g;
+  int rc = resolve(d, &g);
+  if (rc) return rc;
+  if (rows) *rows = g.OH;
+  if (cols) *cols = g.OW;
+  if (planes) *planes = g.pout;
+  return CCT_OK;
+}
+
+static int current_sm100(int *dev) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return set_error(CCT_ENODEV, "no CUDA device visible");
+  }
+  int rc = check_cuda(cudaGetDevice(dev), "cudaGetDevice");
+  if (rc) return rc;
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, *dev);
+  if (major != 10) return set_error(CCT_ENODEV, "device %d is not sm_100 (major %d)", *dev, major);
+  return CCT_OK;
+}
+
+int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
+  if (!out) return set_error(CCT_EINVAL, "null plan output");
+  *out = nullptr;
+  ConvGeom g;
+  int rc = resolve(d, &g);
+  if (rc) return rc;
+  int dev = 0;
+  rc = current_sm100(&dev);
+  if (rc) return rc;
+
+  int algo;
+  const bool reduce = g.mode == CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM ||
+                      g.mode == CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM;
+  if (d->algo == CCT_ALGO_FFT)
+    return set_error(CCT_ENOTSUP, "FFT convolution not available in this build");
+  if (d->precision == CCT_PREC_BF16X3) {
+    if (!reduce)
+      return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
+    return set_error(CCT_ENOTSUP, "BF16X3 frame kernel not available in this build");
+  }
+  algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
+
+  cct_conv_plan *p = new (std::nothrow) cct_conv_plan();
+  if (!p) return set_error(CCT_ENOMEM, "plan allocation failed");
+  p->desc = *d;
+  p->g = g;
+  p->algo = algo;
+  p->device = dev;
+  p->x_elems = (size_t)g.pin * g.H * g.W;
+  p->f_elems = (size_t)g.pf * g.R * g.S;
+  p->y_elems = (size_t)g.pout * g.OH * g.OW;
+  *out = p;
+  return CCT_OK;
+}
+
+int cct_conv_plan_destroy(cct_conv_plan *p) {
+  if (!p) return CCT_OK;
+  cudaFree(p->static_filter);
+  cudaFree(p->d_x);
+  cudaFree(p->d_f);
+  cudaFree(p->d_y);
+  delete p;
+  return CCT_OK;
+}
+
+int cct_conv_plan_algo(const cct_conv_plan *p, int32_t *algo) {
+  if (!p || !algo) return set_error(CCT_EINVAL, "null argument");
+  *algo = p->algo;
+  return CCT_OK;
+}
+
+int cct_conv_plan_set_static_filter(cct_conv_plan *p, const float *host_filter) {
+  if (!p || !host_filter) return set_error(CCT_EINVAL, "null argument");
+  const size_t bytes = p->f_elems * sizeof(float);
+  if (!p->static_filter) {
+    int rc = check_cuda(cudaMalloc(&p->static_filter, bytes), "cudaMalloc(static filter)");
+    if (rc) return rc;
+  }
+  return check_cuda(cudaMemcpy(p->static_filter, host_filter, bytes, cudaMemcpyHostToDevice),
+                    "cudaMemcpy(static filter)");
+}
+
+int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *y, void *stream) {
+  if (!p) return set_error(CCT_EINVAL, "null plan");
+  if (!f) f = p->static_filter;
+  if (!x || !f || !y) return set_error(CCT_EINVAL, "null image, filter or output pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (p->algo) {
+    case ALGO_FRAME_F32:
+      return launch_frame_f32(p->g, x, f, y, st);
+    default:
+      return launch_direct(p->g, x, f, y, st);
+  }
+}
+
+int cct_conv_run_host(cct_conv_plan *p, const float *hx, const float *hf, float *hy, void *stream) {
+  if (!p) return set_error(CCT_EINVAL, "null plan");
+  if (!hx || !hy || (!hf && !p->static_filter))
+    return set_error(CCT_EINVAL, "null host image, filter or output pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  if (!p->d_x) {
+    rc = check_cuda(cudaMalloc(&p->d_x, p->x_elems * sizeof(float)), "cudaMalloc(staging)");
+    if (!rc) rc = check_cuda(cudaMalloc(&p->d_f, p->f_elems * sizeof(float)), "cudaMalloc(staging)");
+    if (!rc) rc = check_cuda(cudaMalloc(&p->d_y, p->y_elems * sizeof(float)), "cudaMalloc(staging)");
+    if (rc) return rc;
+  }
+  rc = check_cuda(cudaMemcpyAsync(p->d_x, hx, p->x_elems * sizeof(float), cudaMemcpyHostToDevice, st),
+                  "H2D image");
+  if (rc) return rc;
+  const float *df = p->static_filter;
+  if (hf) {
+    rc = check_cuda(cudaMemcpyAsync(p->d_f, hf, p->f_elems * sizeof(float), cudaMemcpyHostToDevice, st),
+                    "H2D filter");
+    if (rc) return rc;
+    df = p->d_f;
+  }
+  rc = cct_conv_run(p, p->d_x, df, p->d_y, stream);
+  if (rc) return rc;
+  rc = check_cuda(cudaMemcpyAsync(hy, p->d_y, p->y_elems * sizeof(float), cudaMemcpyDeviceToHost, st),
+                  "D2H output");
+  if (rc) return rc;
+  return check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+}
+
+int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes, const float *x, const float *rf,
+                       int32_t rlen, const float *cf, int32_t clen, int32_t border, int32_t orient,
+                       float *tmp, float *y, void *stream) {
+  if (!x || !rf || !cf || !tmp || !y) return set_error(CCT_EINVAL, "null pointer argument");
+  return launch_separable(rows, cols, planes < 1 ? 1 : planes, x, rf, rlen, cf, clen, border, orient,
+                          tmp, y, (cudaStream_t)stream);
+}
+
+int cct_malloc(void **ptr, size_t bytes) {
+  if (!ptr) return set_error(CCT_EINVAL, "null pointer argument");
+  return check_cuda(cudaMalloc(ptr, bytes), "cudaMalloc");
+}
+int cct_free(void *ptr) { return check_cuda(cudaFree(ptr), "cudaFree"); }
+int cct_memcpy_h2d(void *dst, const void *src, size_t bytes, void *stream) {
+  return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream),
+                    "cudaMemcpyAsync H2D");
+}
+int cct_memcpy_d2h(void *dst, const void *src, size_t bytes, void *stream) {
+  return check_cuda(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream),
+                    "cudaMemcpyAsync D2H");
+}
+int cct_stream_create(void **stream) {
+  if (!stream) return set_error(CCT_EINVAL, "null pointer argument");
+  return check_cuda(cudaStreamCreateWithFlags((cudaStream_t *)stream, cudaStreamNonBlocking),
+                    "cudaStreamCreate");
+}
+int cct_stream_destroy(void *stream) {
+  return check_cuda(cudaStreamDestroy((cudaStream_t)stream), "cudaStreamDestroy");
+}
+int cct_stream_synchronize(void *stream) {
+  return check_cuda(cudaStreamSynchronize((cudaStream_t)stream), "cudaStreamSynchronize");
+}
+
+const char *cct_last_error_string(void) { return g_err; }
+int cct_abi_version(void) { return CCT_ABI_VERSION; }
+uint64_t cct_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+}  // extern "C"

@@ -1,0 +1,86 @@
+// Internal declarations shared by the libcctconv translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "cct_conv.h"
+
+namespace cct {
+
+// Geometry of one ConvolveOp, resolved from a cct_conv_desc.  Coordinates are
+// "post-sampling" (the up-sampled input grid when sampling is UP): output
+// (i, j) reads input rows i*down - low_r + r and cols j*down - low_c + s.
+struct ConvGeom {
+  int H, W;          // input plane (pre-sampling)
+  int OH, OW;        // output plane
+  int R, S;          // filter plane
+  int low_r, low_c;  // low halo (ConvolveHyperKernel.scala:824-830)
+  int border;        // CCT_BORDER_*
+  int orient;        // CCT_CROSS_CORRELATION / CCT_CONVOLUTION
+  int down, up;      // sampling steps (1 when unused)
+  int mode;          // CCT_* vector mode
+  int pin, pf;       // input / filter planes (>= 1)
+  int pout;          // output planes
+  int batch;         // logical images
+  int n;             // planes per image (frame modes)
+  int groups;        // filters per image: pf / n (frame modes)
+  int terms;         // planes summed per output plane (n for *_REDUCE, else 1)
+  uint32_t flags;
+};
+
+// Plane mixing of ConvolveHyperKernel (ConvolveHyperKernel.scala:124-199,
+// 319-340): input and filter plane of term t of output plane o.
+__host__ __device__ inline void plane_pair(const ConvGeom &g, int o, int t,
+                                           int *ip, int *fp) {
+  switch (g.mode) {
+    case CCT_PLANE_BY_PLANE:
+      *ip = g.pin == 1 ? 0 : o;
+      *fp = g.pf == 1 ? 0 : o;
+      break;
+    case CCT_PROJECT_FRAME: {
+      int b = o / g.pf, p = o - b * g.pf;
+      *ip = b * g.n + p % g.n;
+      *fp = p;
+      break;
+    }
+    case CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM: {
+      int b = o / g.groups, k = o - b * g.groups;
+      *ip = b * g.n + t;
+      *fp = k * g.n + t;
+      break;
+    }
+    case CCT_BACK_PROJECT_FRAME: {
+      int b = o / g.pf, w = o - b * g.pf;
+      *ip = b * g.n + w % g.n;
+      *fp = g.groups * (w % g.n) + w / g.n;
+      break;
+    }
+    default: {  // CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM
+      int b = o / g.groups, l = o - b * g.groups;
+      *ip = b * g.n + t;
+      *fp = t * g.groups + l;
+      break;
+    }
+  }
+}
+
+// Error reporting (thread-local message, returned status).
+int set_error(int status, const char *fmt, ...);
+int check_cuda(cudaError_t e, const char *what);
+void count_launches(uint64_t n);
+
+// Kernel families (each returns CCT_OK or an error status).
+int launch_direct(const ConvGeom &g, const float *x, const float *f, float *y,
+                  cudaStream_t stream);
+bool frame_f32_supported(const ConvGeom &g);
+int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
+                     float *y, cudaStream_t stream);
+int launch_separable(int rows, int cols, int planes, const float *x,
+                     const float *rf, int rlen, const float *cf, int clen,
+                     int border, int orient, float *tmp, float *y,
+                     cudaStream_t stream);
+
+}  // namespace cct

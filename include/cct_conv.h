@@ -1,0 +1,170 @@
+/*
+ * cct_conv.h -- C-ABI of the B200 field-convolution backend (libcctconv.so).
+ *
+ * Drop-in replacement for the device half of cct-core's convolution path:
+ * the Scala ComputeGraph keeps building `ConvolveOp` nodes, and the code
+ * generator's `case op: ConvolveOp =>` arm hands them to this library instead
+ * of emitting OpenCL ConvolveHyperKernel/FFT2DHyperKernel text.  Plain C types
+ * only (ints, float pointers, an opaque plan handle, a CUDA stream passed as
+ * void*), so JNI, Panama, ctypes or C++ can bind it unchanged.
+ *
+ * Memory layout (identical to cct-core's FieldMemoryLayoutImpl, so no repack):
+ * a field with P tensor planes of rows x cols is P consecutive pages, each
+ * page row-major with rowStride = cols and no padding
+ * (src/main/scala/cogx/platform/types/FieldMemoryLayoutImpl.scala:250-311).
+ * Frame modes index image plane b*N + c, filter plane k*N + c, fused output
+ * plane b*K + k.
+ *
+ * Errors: every entry point returns CCT_OK (0) or a negative status and never
+ * throws; cct_last_error_string() describes the last failure on the calling
+ * thread.  This replaces the reference's RuntimeException from event status
+ * (src/main/scala/cogx/platform/opencl/OpenCLDeviceKernel.scala:106-147).
+ */
+#ifndef CCT_CONV_H
+#define CCT_CONV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCT_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+  CCT_OK = 0,
+  CCT_EINVAL = -1,    /* descriptor rejected (same rules as the reference)   */
+  CCT_ENOTSUP = -2,   /* legal in the reference, not offered by this build   */
+  CCT_ENOMEM = -3,    /* device or host allocation failed                    */
+  CCT_ECUDA = -4,     /* CUDA runtime / launch error                         */
+  CCT_ETIMEOUT = -5,  /* a bounded device wait gave up                       */
+  CCT_ENODEV = -6     /* no sm_100 device visible                            */
+};
+
+/* ---- policies: numeric values are part of the ABI ----------------------- */
+/* BorderPolicy (src/main/scala/cogx/platform/types/BorderPolicy.scala:30-134) */
+enum { CCT_BORDER_ZERO = 0, CCT_BORDER_CLAMP = 1, CCT_BORDER_CYCLIC = 2,
+       CCT_BORDER_VALID = 3, CCT_BORDER_FULL = 4 };
+/* FilterOrientation (src/main/scala/cogx/platform/types/FilterOrientation.scala:28-30) */
+enum { CCT_CROSS_CORRELATION = 0, CCT_CONVOLUTION = 1 };
+/* ConvolutionSamplingPolicy (src/main/scala/cogx/platform/types/ConvolutionSamplingPolicy.scala:27-31) */
+enum { CCT_SAMPLE_NONE = 0, CCT_SAMPLE_DOWN = 1, CCT_SAMPLE_UP = 2 };
+/* VectorMode (src/main/scala/cogx/compiler/parser/op/BinaryOpcode.scala:36-46) */
+enum { CCT_PLANE_BY_PLANE = 0, CCT_PROJECT_FRAME = 1,
+       CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM = 2, CCT_BACK_PROJECT_FRAME = 3,
+       CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM = 4 };
+/* Arithmetic of the multi-plane (frame) kernels.  FP32 is the reference's
+ * arithmetic; BF16X3 splits each FP32 operand into bf16 hi+lo and sums the
+ * hi*hi + hi*lo + lo*hi products on tcgen05 tensor cores in FP32. */
+enum { CCT_PREC_FP32 = 0, CCT_PREC_BF16X3 = 1 };
+/* Direct vs FFT (ConvolutionFFTUsePolicy.scala:24-28 UseFFTNever/Always/WhenBest) */
+enum { CCT_ALGO_AUTO = 0, CCT_ALGO_DIRECT = 1, CCT_ALGO_FFT = 2 };
+/* flags */
+#define CCT_FLAG_RELU 0x1u   /* fuse max(y, 0) into the store (CogFunctionAPI.scala:109) */
+
+/* ---- descriptor: one ConvolveOp applied to (image, filter) field types ---- */
+typedef struct cct_conv_desc {
+  int32_t struct_size;   /* sizeof(cct_conv_desc), for ABI evolution           */
+  int32_t image_rows;    /* image field shape; 1-D fields use rows = 1         */
+  int32_t image_cols;
+  int32_t image_planes;  /* tensor points; 0 = ScalarField (tensor order 0)    */
+  int32_t filter_rows;
+  int32_t filter_cols;
+  int32_t filter_planes; /* 0 = ScalarField                                    */
+  int32_t batch_size;    /* logical images in the image field (frame modes)    */
+  int32_t border;        /* CCT_BORDER_*                                       */
+  int32_t orientation;   /* CCT_CROSS_CORRELATION / CCT_CONVOLUTION            */
+  int32_t sampling;      /* CCT_SAMPLE_*                                       */
+  int32_t step;          /* sampling step (ignored for CCT_SAMPLE_NONE)        */
+  int32_t vector_mode;   /* CCT_PLANE_BY_PLANE ... BLOCK_REDUCE_SUM            */
+  int32_t precision;     /* CCT_PREC_*                                         */
+  int32_t algo;          /* CCT_ALGO_*                                         */
+  uint32_t flags;        /* CCT_FLAG_*                                         */
+} cct_conv_desc;
+
+typedef struct cct_conv_plan cct_conv_plan;
+
+/* Fill a descriptor with defaults (scalar fields, BorderZero, convolution,
+ * no sampling, plane-by-plane, FP32, AUTO). */
+void cct_conv_desc_init(cct_conv_desc *desc);
+
+/* Output field shape + legality of a descriptor, without touching the GPU.
+ * Replaces ConvolveHyperKernel.outputFieldType
+ * (src/main/scala/cogx/compiler/codegenerator/opencl/hyperkernels/ConvolveHyperKernel.scala:1297-1450)
+ * and the checks of DynamicConvolutionGenerator.convolveDirectly
+ * (src/main/scala/cogx/compiler/codegenerator/opencl/generator/DynamicConvolutionGenerator.scala:484-539). */
+int cct_conv_output_shape(const cct_conv_desc *desc, int32_t *out_rows,
+                          int32_t *out_cols, int32_t *out_planes);
+
+/* Compile-time half of the reference's DynamicConvolutionGenerator.apply
+ * (generator/DynamicConvolutionGenerator.scala:76-150, direct/FFT triage) and
+ * ConvolveHyperKernel.apply (hyperkernels/ConvolveHyperKernel.scala:1003-1148,
+ * parameter choice): validates, picks the kernel family and tile shape for
+ * the current device, and allocates every device buffer the plan needs so
+ * that cct_conv_run allocates nothing. */
+int cct_conv_plan_create(const cct_conv_desc *desc, cct_conv_plan **plan);
+int cct_conv_plan_destroy(cct_conv_plan *plan);
+
+/* Kernel family the plan chose: 0 direct stencil, 1 frame FP32, 2 frame
+ * BF16X3 tensor core, 3 FFT. */
+int cct_conv_plan_algo(const cct_conv_plan *plan, int32_t *algo_out);
+
+/* Static filter (the reference's ConstantFieldKernel filter): its FFT
+ * spectrum, or its packed tensor-core operand, is computed once here in
+ * FP64 / on the device, as the reference does on the host at compile time
+ * (generator/DynamicConvolutionGenerator.scala:342-350, 376-405).  After this
+ * call cct_conv_run accepts filter == NULL.  host_filter holds
+ * filter_planes x filter_rows x filter_cols floats. */
+int cct_conv_plan_set_static_filter(cct_conv_plan *plan, const float *host_filter);
+
+/* One step of the op: device pointers in the planar layout above, enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream).  Replaces the
+ * per-step launch OpenCLDeviceKernel.phase1Clock -> put{2,3}DRangeKernel
+ * (src/main/scala/cogx/platform/opencl/OpenCLDeviceKernel.scala:67-104,
+ * 189-215).  Asynchronous; allocates nothing.  filter may be NULL after
+ * cct_conv_plan_set_static_filter. */
+int cct_conv_run(const cct_conv_plan *plan, const float *image,
+                 const float *filter, float *out, void *stream);
+
+/* The same step with HOST buffers: pinned staging + device copies owned by
+ * the plan, H2D of image (and filter unless static), the kernel, D2H of the
+ * result, then a stream synchronise.  What a JNI caller holding Java direct
+ * buffers uses in place of OpenCLBuffer.write/read
+ * (src/main/scala/cogx/platform/opencl/OpenCLBuffer.scala:207-230). */
+int cct_conv_run_host(cct_conv_plan *plan, const float *host_image,
+                      const float *host_filter, float *host_out, void *stream);
+
+/* Separable convolution: rows pass then columns pass, BorderZero / Clamp /
+ * Cyclic, odd 1-D filters, every plane of the image.  Replaces
+ * ConvolveRows2DHyperKernel + ConvolveColumns2DHyperKernel
+ * (hyperkernels/ConvolveRows2DHyperKernel.scala:37-160,
+ * hyperkernels/ConvolveColumns2DHyperKernel.scala:37-160) behind
+ * convolveSeparable / crossCorrelateSeparable (api/CogFunctionAPI.scala:1277-1366).
+ * tmp is a device buffer of planes*rows*cols floats. */
+int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes,
+                       const float *image, const float *row_filter,
+                       int32_t row_len, const float *col_filter,
+                       int32_t col_len, int32_t border, int32_t orientation,
+                       float *tmp, float *out, void *stream);
+
+/* ---- device memory helpers (the JNI side has no CUDA runtime) ----------- */
+int cct_malloc(void **ptr, size_t bytes);
+int cct_free(void *ptr);
+int cct_memcpy_h2d(void *dst, const void *src, size_t bytes, void *stream);
+int cct_memcpy_d2h(void *dst, const void *src, size_t bytes, void *stream);
+int cct_stream_create(void **stream);
+int cct_stream_destroy(void *stream);
+int cct_stream_synchronize(void *stream);
+
+/* ---- diagnostics --------------------------------------------------------- */
+const char *cct_last_error_string(void);
+int cct_abi_version(void);
+/* Kernel launches issued by this process so far (all plans, all threads). */
+uint64_t cct_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CCT_CONV_H */

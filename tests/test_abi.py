@@ -1,0 +1,108 @@
+"""libcctconv.so loads, exports every declared symbol, and its host-side
+descriptor logic agrees with the oracle's restatement (no GPU needed)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle as O
+from cctconv import _lib
+
+HEADERS = sorted((Path(__file__).resolve().parent.parent / "include").glob("*.h"))
+
+
+def declared_functions():
+    names = []
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names += re.findall(r"^[A-Za-z_][\w \*]*?\b(cct_\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(_lib.LIB, n), n
+        assert n in _lib.SIGNATURES, f"{n} not bound in cctconv._lib"
+
+
+def test_abi_version_and_desc_size():
+    assert _lib.LIB.cct_abi_version() == 1
+    d = _lib.new_desc()
+    assert d.struct_size == ctypes.sizeof(_lib.ConvDesc) == 64
+    assert d.batch_size == 1 and d.orientation == _lib.CONVOLUTION
+
+
+def _oracle_desc(d):
+    return O.make_desc(d.image_rows, d.image_cols, d.filter_rows, d.filter_cols,
+                       planes=d.image_planes, f_planes=d.filter_planes, batch=d.batch_size,
+                       border=d.border, orient=d.orientation, sampling=d.sampling, step=d.step,
+                       mode=d.vector_mode)
+
+
+def test_output_shape_agrees_with_oracle_on_random_descriptors():
+    rng = np.random.default_rng(1234)
+    n_ok = n_err = 0
+    for _ in range(4000):
+        d = _lib.new_desc(
+            image_rows=int(rng.integers(1, 40)), image_cols=int(rng.integers(1, 40)),
+            image_planes=int(rng.choice([0, 1, 2, 3, 4, 6, 8, 12])),
+            filter_rows=int(rng.integers(1, 10)), filter_cols=int(rng.integers(1, 10)),
+            filter_planes=int(rng.choice([0, 1, 2, 3, 4, 6, 8, 12, 24])),
+            batch_size=int(rng.choice([1, 2, 3, 4])), border=int(rng.integers(0, 5)),
+            orientation=int(rng.integers(0, 2)), sampling=int(rng.integers(0, 3)),
+            step=int(rng.integers(1, 5)), vector_mode=int(rng.integers(0, 5)))
+        try:
+            want = O.output_shape(_oracle_desc(d))
+        except ValueError:
+            want = None
+        try:
+            got = _lib.output_shape(d)
+        except _lib.CctError as e:
+            assert e.status == _lib.EINVAL
+            got = None
+        assert got == want, (d.key(), got, want)
+        n_ok += got is not None
+        n_err += got is None
+    assert n_ok > 500 and n_err > 500
+
+
+@pytest.mark.parametrize("field,expect", [
+    (dict(struct_size=12), "struct_size"),
+    (dict(border=9), "bad border"),
+    (dict(precision=7), "bad precision"),
+    (dict(flags=0x10), "unknown flags"),
+    (dict(filter_rows=4, filter_cols=3), "odd shape"),
+])
+def test_invalid_descriptors_report_einval(field, expect):
+    d = _lib.new_desc(image_rows=16, image_cols=16, filter_rows=3, filter_cols=3)
+    for k, v in field.items():
+        setattr(d, k, v)
+    with pytest.raises(_lib.CctError, match=expect) as e:
+        _lib.output_shape(d)
+    assert e.value.status == _lib.EINVAL
+
+
+def test_reference_error_messages():
+    d = _lib.new_desc(image_rows=10, image_cols=10, filter_rows=3, filter_cols=3,
+                      border=_lib.BORDER_CLAMP, sampling=_lib.SAMPLE_UP, step=2)
+    with pytest.raises(_lib.CctError, match="Integrated upsampling with BorderClamp"):
+        _lib.output_shape(d)
+    d = _lib.new_desc(image_rows=11, image_cols=10, filter_rows=3, filter_cols=3,
+                      sampling=_lib.SAMPLE_DOWN, step=2)
+    with pytest.raises(_lib.CctError, match="divisible by the downsampling step"):
+        _lib.output_shape(d)
+
+
+def test_plan_without_gpu_is_enodev():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    d = _lib.new_desc(image_rows=16, image_cols=16, filter_rows=3, filter_cols=3)
+    with pytest.raises(_lib.CctError) as e:
+        _lib.Plan(d)
+    assert e.value.status == _lib.ENODEV

@@ -1,0 +1,216 @@
+"""The CPU oracle pinned against the reference's own golden vectors and
+known-answer tests (no GPU).
+
+Golden vectors: src/test/resources/platform/opencl/hyperkernels/convolutionDynamic/
+(25 cases, read by src/test/scala/cogx/DynamicConvolutionSpec.scala:131-203).
+Known answers: src/test/scala/cogx/StaticConvolutionSpec.scala:36-236.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from helpers import (ADJOINT_BORDER, ADJOINT_SAMPLING, golden_case, legal_in_reference,
+                     ref_field_approx_equal)
+
+
+@pytest.mark.parametrize("i", range(25))
+def test_golden_forward(golden, i):
+    """convolve(x, k, border, sampling) ~== wx, as DynamicConvolutionSpec checks."""
+    sampling, step, border, a = golden_case(golden, i)
+    x, k, wx = a["x"], a["k"], a["wx"]
+    desc = O.make_desc(x.shape[0], x.shape[1], k.shape[0], k.shape[1], border=border,
+                       orient=O.CONV, sampling=sampling, step=step)
+    if not legal_in_reference(sampling, step, border):
+        with pytest.raises(ValueError, match="upsampling with BorderClamp"):
+            O.output_shape(desc)
+        return
+    assert O.output_shape(desc) == (wx.shape[0], wx.shape[1], 1)
+    y32 = O.conv(desc, x, k)[0]
+    y64 = O.conv(desc, x, k, np.float64)[0]
+    assert ref_field_approx_equal(y32, wx)
+    # the golden values are float32 roundings of the exact result
+    assert np.max(np.abs(y64 - wx)) < 5e-7
+    assert O.rel_errors(y32, y64)[0] < 2e-7
+
+
+@pytest.mark.parametrize("i", range(25))
+def test_golden_adjoint(golden, i):
+    """wty is the adjoint applied to y: crossCorrelate with the adjoint border
+    and the reverse sampling (these files ship with the reference but no test
+    of it reads them)."""
+    sampling, step, border, a = golden_case(golden, i)
+    if border not in ADJOINT_BORDER:
+        pytest.skip("BorderClamp has no convolution-form adjoint")
+    y, k, wty = a["y"], a["k"], a["wty"]
+    desc = O.make_desc(y.shape[0], y.shape[1], k.shape[0], k.shape[1],
+                       border=ADJOINT_BORDER[border], orient=O.XCORR,
+                       sampling=ADJOINT_SAMPLING[sampling], step=step)
+    assert O.output_shape(desc)[:2] == wty.shape
+    got = O.conv(desc, y, k, np.float64)[0]
+    assert np.max(np.abs(got - wty)) < 5e-7
+
+
+def _run2d(img, ker, border, orient):
+    desc = O.make_desc(img.shape[0], img.shape[1], ker.shape[0], ker.shape[1], border=border,
+                       orient=orient)
+    return O.conv(desc, img, ker)[0]
+
+
+KERNEL = np.array([[0.25, 0.50, 0.25], [0.50, 1.00, 0.50], [0.25, 0.50, 0.25]], np.float32)
+IMAGE = np.array([[0, 1, 2, 3], [2, 3, 4, 5], [8, 7, 6, 4], [5, 4, 9, 8]], np.float32)
+
+
+def test_known_answer_1d():
+    """StaticConvolutionSpec.scala:62-87 ("scalar convolve scalar, 1D")."""
+    img = np.array([[1, 2, 3, 4]], np.float32)
+    ker = np.array([[0.25, 0.5, 0.25]], np.float32)
+    assert np.allclose(_run2d(img, ker, O.CLAMP, O.CONV), [[1.25, 2.0, 3.0, 3.75]])
+    assert np.allclose(_run2d(img, ker, O.CYCLIC, O.CONV), [[2.0, 2.0, 3.0, 3.0]])
+    assert np.allclose(_run2d(img, ker, O.ZERO, O.CONV), [[1.0, 2.0, 3.0, 2.75]])
+
+
+def test_known_answer_2d():
+    """StaticConvolutionSpec.scala:89-127 and :182-204."""
+    clamp = [[3.0, 6.0, 10.0, 13.0], [12.5, 14.0, 15.75, 16.75],
+             [22.5, 22.5, 23.0, 22.0], [22.0, 23.5, 28.25, 29.25]]
+    cyclic = [[10.5, 10.5, 15.5, 15.5], [13.75, 14.0, 15.75, 15.50],
+              [22.0, 22.5, 23.0, 22.5], [18.75, 19.0, 22.75, 22.5]]
+    zero = [[2.25, 5.0, 8.0, 7.5], [9.5, 14.0, 15.75, 12.5],
+            [16.75, 22.5, 23.0, 16.75], [12.75, 18.0, 20.75, 16.0]]
+    assert np.array_equal(_run2d(IMAGE, KERNEL, O.CLAMP, O.CONV), np.float32(clamp))
+    assert np.array_equal(_run2d(IMAGE, KERNEL, O.CYCLIC, O.CONV), np.float32(cyclic))
+    assert np.array_equal(_run2d(IMAGE, KERNEL, O.ZERO, O.CONV), np.float32(zero))
+
+
+def test_known_answer_xcorr():
+    """StaticConvolutionSpec.scala:206-236 ("scalar cross-correlate scalar, 2D")."""
+    ker = np.float32([[1, 2, 0], [0, 3, 0], [0, 0, 0]])
+    want = np.float32([[0, 5, 11, 17], [6, 11, 17, 23], [30, 29, 29, 26], [39, 34, 46, 38]])
+    assert np.array_equal(_run2d(IMAGE, ker, O.CLAMP, O.XCORR), want)
+
+
+@pytest.mark.parametrize("border", [O.ZERO, O.CLAMP, O.CYCLIC])
+def test_separable_equals_full(border):
+    """DynamicConvolutionSpec.scala:75-109: separable == full 2-D filter."""
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-1, 1, (10, 10)).astype(np.float32)
+    row = np.float32([0.1, 0.3, 0.4, 0.2, 0.0])
+    col = np.float32([0.0, 0.5, -0.4, -0.2, -0.1])
+    full = np.outer(col, row).astype(np.float32)
+    for orient in (O.CONV, O.XCORR):
+        sep = O.separable(x, row, col, border, orient)
+        ref = _run2d(x, full, border, orient)
+        assert np.max(np.abs(sep - ref)) < 1e-5
+
+
+def test_fft64_matches_direct64():
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0, 1, (64, 32))
+    f = rng.uniform(-1, 1, (7, 5))
+    desc = O.make_desc(64, 32, 7, 5, border=O.CYCLIC, orient=O.CONV)
+    direct = O.conv(desc, x, f, np.float64)[0]
+    assert np.max(np.abs(O.cyclic_conv_fft64(x, f, O.CONV) - direct)) < 1e-12
+
+
+SHAPE_CASES = [
+    # (rows, cols, fr, fc, border, sampling, step) -> (orows, ocols) or error text
+    ((64, 64, 5, 5, O.ZERO, O.NOSAMPLE, 1), (64, 64)),
+    ((64, 64, 5, 5, O.VALID, O.NOSAMPLE, 1), (60, 60)),
+    ((64, 64, 5, 5, O.FULL, O.NOSAMPLE, 1), (68, 68)),
+    ((64, 64, 3, 3, O.ZERO, O.DOWN, 2), (32, 32)),
+    ((65, 64, 3, 3, O.ZERO, O.DOWN, 2), "divisible by the downsampling step"),
+    ((61, 61, 6, 6, O.VALID, O.DOWN, 4), (14, 14)),
+    ((10, 12, 3, 3, O.ZERO, O.UP, 3), (30, 36)),
+    ((10, 12, 3, 3, O.CLAMP, O.UP, 3), "upsampling with BorderClamp"),
+    ((10, 12, 3, 3, O.CLAMP, O.UP, 1), (10, 12)),
+    ((10, 12, 4, 3, O.ZERO, O.NOSAMPLE, 1), "odd shape"),
+    ((10, 12, 4, 3, O.FULL, O.NOSAMPLE, 1), (13, 14)),
+    ((4, 4, 5, 5, O.VALID, O.NOSAMPLE, 1), "larger than the input"),
+]
+
+
+@pytest.mark.parametrize("args,want", SHAPE_CASES)
+def test_output_shape_rules(args, want):
+    rows, cols, fr, fc, border, sampling, step = args
+    desc = O.make_desc(rows, cols, fr, fc, border=border, sampling=sampling, step=step)
+    if isinstance(want, str):
+        with pytest.raises(ValueError, match=want):
+            O.output_shape(desc)
+    else:
+        assert O.output_shape(desc)[:2] == want
+
+
+def test_frame_plane_counts():
+    # projectFrame: B*F planes; fused: B*K; backProjectFrame: B*F; fused: B*L
+    d = O.make_desc(8, 8, 3, 3, planes=16 * 32, f_planes=64 * 32, batch=16, mode=O.PROJECT)
+    assert O.output_shape(d)[2] == 16 * 64 * 32
+    d.mode = O.PROJECT_REDUCE
+    assert O.output_shape(d)[2] == 16 * 64
+    d = O.make_desc(8, 8, 3, 3, planes=16 * 64, f_planes=64 * 32, batch=16, mode=O.BACKPROJECT_REDUCE)
+    assert O.output_shape(d)[2] == 16 * 32
+    d = O.make_desc(8, 8, 3, 3, planes=30, f_planes=64, batch=16, mode=O.PROJECT)
+    with pytest.raises(ValueError, match="multiple of the batch"):
+        O.output_shape(d)
+    d = O.make_desc(8, 8, 3, 3, planes=3, f_planes=4, mode=O.PLANE)
+    with pytest.raises(ValueError, match="plane-by-plane"):
+        O.output_shape(d)
+
+
+def _plane_xcorr64(x, f, border=O.ZERO, orient=O.XCORR):
+    return O.conv(O.make_desc(x.shape[0], x.shape[1], f.shape[0], f.shape[1], border=border,
+                              orient=orient), x, f, np.float64)[0]
+
+
+def test_frame_semantics_by_composition():
+    """projectFrame / backProjectFrame index semantics pinned by plane-wise
+    compositions, as StaticConvolutionSpec.scala:536-584 and :1653-1905 do."""
+    rng = np.random.default_rng(11)
+    B, N, K, H, W, R = 2, 3, 4, 9, 7, 3
+    x = rng.normal(size=(B * N, H, W))
+    f = rng.normal(size=(K * N, R, R))
+    # projectFrame
+    d = O.make_desc(H, W, R, R, planes=B * N, f_planes=K * N, batch=B, orient=O.XCORR, mode=O.PROJECT)
+    y = O.conv(d, x, f, np.float64)
+    for b in range(B):
+        for p in range(K * N):
+            assert np.allclose(y[b * K * N + p], _plane_xcorr64(x[b * N + p % N], f[p]))
+    # fused projectFrame
+    d.mode = O.PROJECT_REDUCE
+    y = O.conv(d, x, f, np.float64)
+    for b in range(B):
+        for k in range(K):
+            ref = sum(_plane_xcorr64(x[b * N + c], f[k * N + c]) for c in range(N))
+            assert np.allclose(y[b * K + k], ref)
+    # backProjectFrame: image planes N per image, L = F / N logical filters
+    d = O.make_desc(H, W, R, R, planes=B * N, f_planes=K * N, batch=B, orient=O.CONV, mode=O.BACKPROJECT)
+    y = O.conv(d, x, f, np.float64)
+    L = K
+    for b in range(B):
+        for w in range(K * N):
+            ref = _plane_xcorr64(x[b * N + w % N], f[L * (w % N) + w // N], orient=O.CONV)
+            assert np.allclose(y[b * K * N + w], ref)
+    d.mode = O.BACKPROJECT_REDUCE
+    y = O.conv(d, x, f, np.float64)
+    for b in range(B):
+        for l in range(L):
+            ref = sum(_plane_xcorr64(x[b * N + n], f[n * L + l], orient=O.CONV) for n in range(N))
+            assert np.allclose(y[b * L + l], ref)
+
+
+def test_fused_backproject_is_adjoint_of_projectframe():
+    """<projectFrame(x), g> == <x, backProjectFrame(g)> for BorderZero."""
+    rng = np.random.default_rng(5)
+    B, C, K, H, W, R = 2, 3, 5, 8, 6, 5
+    x = rng.normal(size=(B * C, H, W))
+    g = rng.normal(size=(B * K, H, W))
+    f = rng.normal(size=(K * C, R, R))
+    fwd = O.conv(O.make_desc(H, W, R, R, planes=B * C, f_planes=K * C, batch=B, orient=O.XCORR,
+                             mode=O.PROJECT_REDUCE), x, f, np.float64)
+    bwd = O.conv(O.make_desc(H, W, R, R, planes=B * K, f_planes=K * C, batch=B, orient=O.CONV,
+                             mode=O.BACKPROJECT_REDUCE), g, f, np.float64)
+    assert abs(np.sum(fwd * g) - np.sum(x * bwd)) < 1e-9 * np.sum(np.abs(fwd * g))
+
+
+def test_poor_float_semantics():
+    assert O.poor_float_equal([1.0, 0.0], [1.0 + 1e-4, 1e-3])
+    assert not O.poor_float_equal([1.0], [1.01])

@@ -32,8 +32,8 @@ GFLOP_FRAME = 2 * 16 * 64 * 64 * 64 * 32 * 5 * 5 / 1e9  # 6.711 per direction
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["frame", "plain", "separable"], default="frame")
     ap.add_argument("--precision", choices=["auto", "fp32", "bf16x3"], default="auto")
@@ -96,6 +96,7 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        time.sleep(1.0)  # let nvidia-smi start sampling before the timed region
         return self
 
     def __exit__(self, *exc):
@@ -231,7 +232,7 @@ def plain_workload():
         "config": {"workload": "plain convolve 256x256 (*) 5x5 BorderZero, 4096 planes per launch",
                    "planes": P, "H": H, "W": W, "R": R, "l2": "1 GiB input > 126 MB L2"},
         "dtype": "f32", "keep": (plan, plan64, x, y, f, hx, hy, hf),
-        "kernel": "direct_fixed_kernel", "bytes_per_launch": byts,
+        "kernel": "direct_tma_kernel", "bytes_per_launch": byts,
     }
 
 
@@ -385,9 +386,9 @@ def main():
     t_max = max_over_ranks(pg, elapsed)
 
     per_launch = time_single_launch(wl["launch_single"])
-    e2e_t, _ = time_steps(wl["e2e_step"], max(args.steps // 5, 3), 2, pg)
+    e2e_t, _ = time_steps(wl["e2e_step"], max(args.steps // 20, 3), 2, pg)
     e2e_t = max_over_ranks(pg, e2e_t)
-    e2e_steps = max(args.steps // 5, 3)
+    e2e_steps = max(args.steps // 20, 3)
 
     if wl["unit"] == "GFLOP/s":
         value = world * wl["gflop_per_step"] * args.steps / t_max

@@ -77,6 +77,7 @@ SIGNATURES = {
     "cct_stream_create": (_I, [ctypes.POINTER(_P)]),
     "cct_stream_destroy": (_I, [_P]),
     "cct_stream_synchronize": (_I, [_P]),
+    "cct_device_status": (_I, []),
     "cct_last_error_string": (ctypes.c_char_p, []),
     "cct_abi_version": (_I, []),
     "cct_launch_count": (ctypes.c_uint64, []),

@@ -5,6 +5,7 @@
 // DynamicConvolutionGenerator.convolveDirectly
 // (generator/DynamicConvolutionGenerator.scala:484-539).
 #include <atomic>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +34,25 @@ int check_cuda(cudaError_t e, const char *what) {
 }
 
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+static std::mutex g_err_mu;
+static unsigned *g_err_word[64];
+
+unsigned *device_error_word() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(g_err_mu);
+  if (!g_err_word[dev]) {
+    unsigned *p = nullptr;
+    if (cudaMalloc(&p, sizeof(unsigned)) != cudaSuccess) return nullptr;
+    if (cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess) {
+      cudaFree(p);
+      return nullptr;
+    }
+    g_err_word[dev] = p;
+  }
+  return g_err_word[dev];
+}
 
 // Resolve and validate a descriptor.  Returns CCT_OK or CCT_EINVAL with the
 // reference's error text.
@@ -151,6 +171,7 @@ struct cct_conv_plan {
   ConvGeom g;
   int algo;
   int device;
+  unsigned *err;  // device error word of `device`
   size_t x_elems, f_elems, y_elems;
   float *static_filter;  // device copy of a static filter, or null
   // run_host staging (allocated on the first cct_conv_run_host call)
@@ -222,12 +243,16 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   }
   algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
 
+  unsigned *err_word = device_error_word();
+  if (!err_word) return set_error(CCT_ENOMEM, "device error word allocation failed");
+
   cct_conv_plan *p = new (std::nothrow) cct_conv_plan();
   if (!p) return set_error(CCT_ENOMEM, "plan allocation failed");
   p->desc = *d;
   p->g = g;
   p->algo = algo;
   p->device = dev;
+  p->err = err_word;
   p->x_elems = (size_t)g.pin * g.H * g.W;
   p->f_elems = (size_t)g.pf * g.R * g.S;
   p->y_elems = (size_t)g.pout * g.OH * g.OW;
@@ -271,6 +296,7 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);
     default:
+      if (direct_tma_supported(p->g, x)) return launch_direct_tma(p->g, x, f, y, st, p->err);
       return launch_direct(p->g, x, f, y, st);
   }
 }
@@ -336,6 +362,17 @@ int cct_stream_destroy(void *stream) {
 }
 int cct_stream_synchronize(void *stream) {
   return check_cuda(cudaStreamSynchronize((cudaStream_t)stream), "cudaStreamSynchronize");
+}
+
+int cct_device_status(void) {
+  unsigned *w = device_error_word();
+  if (!w) return set_error(CCT_ENODEV, "no device error word");
+  unsigned v = 0;
+  int rc = check_cuda(cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost), "cudaMemcpy(status)");
+  if (rc) return rc;
+  if (v == 0) return CCT_OK;
+  cudaMemset(w, 0, sizeof(unsigned));
+  return set_error(CCT_ETIMEOUT, "a bounded wait inside a kernel gave up (status 0x%x)", v);
 }
 
 const char *cct_last_error_string(void) { return g_err; }

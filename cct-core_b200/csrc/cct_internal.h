@@ -75,6 +75,12 @@ void count_launches(uint64_t n);
 // Kernel families (each returns CCT_OK or an error status).
 int launch_direct(const ConvGeom &g, const float *x, const float *f, float *y,
                   cudaStream_t stream);
+bool direct_tma_supported(const ConvGeom &g, const float *x);
+int launch_direct_tma(const ConvGeom &g, const float *x, const float *f, float *y,
+                      cudaStream_t stream, unsigned *err);
+// Per-device error word passed to kernels with bounded waits (allocated on
+// first use on the current device).
+unsigned *device_error_word();
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);

@@ -159,6 +159,13 @@ int cct_stream_destroy(void *stream);
 int cct_stream_synchronize(void *stream);
 
 /* ---- diagnostics --------------------------------------------------------- */
+/* Device-side status of this library's kernels on the current device since
+ * the last call: CCT_OK, or CCT_ETIMEOUT when a bounded wait inside a kernel
+ * gave up (that kernel returned early and its output is undefined).  The
+ * reference surfaces device failures as a CLEvent error status
+ * (src/main/scala/cogx/platform/opencl/OpenCLDeviceKernel.scala:106-147).
+ * Reading clears the status; the call synchronises with the device. */
+int cct_device_status(void);
 const char *cct_last_error_string(void);
 int cct_abi_version(void);
 /* Kernel launches issued by this process so far (all plans, all threads). */

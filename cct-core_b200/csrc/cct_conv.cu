@@ -13,6 +13,7 @@
 #include <new>
 
 #include "cct_internal.h"
+#include "frame_tc.h"
 
 namespace cct {
 
@@ -174,6 +175,9 @@ struct cct_conv_plan {
   unsigned *err;  // device error word of `device`
   size_t x_elems, f_elems, y_elems;
   float *static_filter;  // device copy of a static filter, or null
+  TcParams tc;           // tensor-core tile plan (ALGO_FRAME_BF16X3)
+  uint8_t *packed;       // packed bf16 hi/lo filter operand (plan workspace)
+  bool packed_static;    // packed holds the static filter
   // run_host staging (allocated on the first cct_conv_run_host call)
   float *d_x, *d_f, *d_y;
 };
@@ -236,12 +240,15 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
                       g.mode == CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM;
   if (d->algo == CCT_ALGO_FFT)
     return set_error(CCT_ENOTSUP, "FFT convolution not available in this build");
-  if (d->precision == CCT_PREC_BF16X3) {
-    if (!reduce)
-      return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
-    return set_error(CCT_ENOTSUP, "BF16X3 frame kernel not available in this build");
-  }
-  algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
+  TcParams tc{};
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (d->precision == CCT_PREC_BF16X3 && !reduce)
+    return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
+  if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
+    algo = ALGO_FRAME_BF16X3;
+  else
+    algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
 
   unsigned *err_word = device_error_word();
   if (!err_word) return set_error(CCT_ENOMEM, "device error word allocation failed");
@@ -256,6 +263,14 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   p->x_elems = (size_t)g.pin * g.H * g.W;
   p->f_elems = (size_t)g.pf * g.R * g.S;
   p->y_elems = (size_t)g.pout * g.OH * g.OW;
+  p->tc = tc;
+  if (algo == ALGO_FRAME_BF16X3) {
+    rc = check_cuda(cudaMalloc(&p->packed, tc.pack_bytes), "cudaMalloc(packed filters)");
+    if (rc) {
+      delete p;
+      return rc;
+    }
+  }
   *out = p;
   return CCT_OK;
 }
@@ -263,6 +278,7 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
 int cct_conv_plan_destroy(cct_conv_plan *p) {
   if (!p) return CCT_OK;
   cudaFree(p->static_filter);
+  cudaFree(p->packed);
   cudaFree(p->d_x);
   cudaFree(p->d_f);
   cudaFree(p->d_y);
@@ -283,8 +299,16 @@ int cct_conv_plan_set_static_filter(cct_conv_plan *p, const float *host_filter) 
     int rc = check_cuda(cudaMalloc(&p->static_filter, bytes), "cudaMalloc(static filter)");
     if (rc) return rc;
   }
-  return check_cuda(cudaMemcpy(p->static_filter, host_filter, bytes, cudaMemcpyHostToDevice),
-                    "cudaMemcpy(static filter)");
+  int rc = check_cuda(cudaMemcpy(p->static_filter, host_filter, bytes, cudaMemcpyHostToDevice),
+                      "cudaMemcpy(static filter)");
+  if (rc) return rc;
+  if (p->algo == ALGO_FRAME_BF16X3) {
+    rc = launch_pack_filters(p->tc, p->static_filter, p->packed, 0);
+    if (!rc) rc = check_cuda(cudaStreamSynchronize(0), "pack static filter");
+    if (rc) return rc;
+    p->packed_static = true;
+  }
+  return CCT_OK;
 }
 
 int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *y, void *stream) {
@@ -293,6 +317,14 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
   if (!x || !f || !y) return set_error(CCT_EINVAL, "null image, filter or output pointer");
   cudaStream_t st = (cudaStream_t)stream;
   switch (p->algo) {
+    case ALGO_FRAME_BF16X3: {
+      if ((reinterpret_cast<uintptr_t>(x) & 15) != 0)
+        return set_error(CCT_EINVAL, "image pointer must be 16-byte aligned for the tensor-core path");
+      int rc = CCT_OK;
+      if (f != p->static_filter || !p->packed_static) rc = launch_pack_filters(p->tc, f, p->packed, st);
+      if (rc) return rc;
+      return launch_frame_tc(p->tc, x, y, p->packed, p->err, st);
+    }
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);
     default:

@@ -235,11 +235,16 @@ int launch_tma(const ConvGeom &g, const float *x, const float *f, float *y, cuda
 
 int encode_tensor_map_3d(CUtensorMap *map, const float *base, uint64_t cols, uint64_t rows,
                          uint64_t planes, uint32_t box_c, uint32_t box_r) {
+  return encode_tensor_map_3d_box(map, base, cols, rows, planes, box_c, box_r, 1);
+}
+
+int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols, uint64_t rows,
+                             uint64_t planes, uint32_t box_c, uint32_t box_r, uint32_t box_z) {
   EncodeFn fn = encode_fn();
   if (!fn) return set_error(CCT_ECUDA, "cuTensorMapEncodeTiled unavailable");
   const cuuint64_t dims[3] = {cols, rows, planes};
   const cuuint64_t strides[2] = {cols * 4, cols * rows * 4};
-  const cuuint32_t box[3] = {box_c, box_r, 1};
+  const cuuint32_t box[3] = {box_c, box_r, box_z};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *)base, dims, strides, box, estr,
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -1,0 +1,430 @@
+// Fused filter-bank convolution (ProjectFrame / BackProjectFrame with the
+// BlockReduceSum fused, ConvolveHyperKernel.scala:153-199, 319-340, 574-645)
+// as an implicit GEMM on the tcgen05 tensor cores, in split-BF16 precision:
+//   x = xh + xl, f = fh + fl (bf16 hi + bf16 residual), and
+//   y = sum xh*fh + xh*fl + xl*fh   accumulated in FP32 in tensor memory.
+//
+// GEMM view per image b: D[pixel m][filter n] = sum over (plane c, tap r,s)
+//   A[m][c,r,s] * B[n][c,r,s],  A = im2col of the input planes, B = filters.
+// The reduction walks "chunks": one filter tap x CB input planes.
+//
+// Warp roles (persistent CTAs, one per SM):
+//   warps 0-3  producers: one output pixel per lane; read the CB plane values
+//              of the pixel's tap from the shared-memory halo tile, split
+//              them into bf16 hi/lo and store them to tensor memory as the
+//              A operand (tcgen05.st, row m = lane m).
+//   warp  4    MMA issuer: per chunk 3 x CB/16 tcgen05.mma (A from tensor
+//              memory, B from shared memory) into a double-buffered FP32
+//              accumulator in tensor memory.
+//   warp  5    loader: 3-D TMA loads of the halo tile (zero fill at the
+//              border) and bulk copies of the pre-packed filter chunks.
+//   warps 6-9  epilogue: tcgen05.ld of the accumulator, optional ReLU,
+//              coalesced stores to the output planes.
+// Every mbarrier wait is bounded; on a timeout the CTA raises the device
+// error word, lets in-flight copies land, frees its tensor memory and exits.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <mutex>
+#include <unordered_map>
+
+#include "cct_internal.h"
+#include "frame_tc.h"
+#include "sm100_util.cuh"
+
+namespace cct {
+namespace {
+
+constexpr int kMT = 128;        // output pixels per tile (MMA M)
+constexpr int kStages = 8;      // A/B chunk pipeline depth
+constexpr int kThreads = 320;   // 10 warps
+constexpr int kMmaWarp = 4, kLoadWarp = 5;  // warps 6-9: epilogue
+
+// Byte offset of element (n, k) inside one packed K-major operand image of
+// rows x CB bf16 (no swizzle): core matrix (8 rows x 8 elements, 128 bytes)
+// at (n/8)*SBO + (k/8)*LBO, LBO = 128, SBO = CB*16.
+__host__ __device__ inline uint32_t packed_offset(int n, int k, int CB) {
+  return (uint32_t)((n >> 3) * (CB * 16) + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2);
+}
+
+struct Barriers {
+  uint64_t full[kStages], empty[kStages];
+  uint64_t hfull[2], hempty[2];
+  uint64_t dfull[2], dempty[2];
+  uint32_t tmem_slot;
+  int abort_flag;
+};
+
+template <int CB>
+__global__ void __launch_bounds__(kThreads, 1)
+    frame_tc_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ TcParams p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ Barriers bars;
+  const ConvGeom &g = p.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  auto halo_buf = [&](int h) { return smem + (h ? p.halo_bytes : 0u); };
+  uint8_t *bstage = smem + 2 * p.halo_bytes;
+  const uint32_t bstage_bytes = 2u * p.NT * CB * 2;  // hi + lo images
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&bars.full[s], 129);  // 128 producer arrivals + loader expect_tx
+      mbar_init(&bars.empty[s], 1);   // MMA commit
+    }
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&bars.hfull[h], 1);
+      mbar_init(&bars.hempty[h], 128);
+      mbar_init(&bars.dfull[h], 1);
+      mbar_init(&bars.dempty[h], 128);
+    }
+    bars.abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == kMmaWarp) tmem_alloc(&bars.tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = bars.tmem_slot;
+
+  const int RS = g.R * g.S;
+  const int npix = g.OH * g.OW;
+  auto d_col = [&](int d) { return d ? (uint32_t)p.NT : 0u; };
+  const uint32_t a_col0 = 2u * p.NT;  // stage s: hi at a_col0 + s*CB, lo at + CB/2
+  volatile int *abort_flag = &bars.abort_flag;
+
+  auto tile_decode = [&](int i, int &b, int &mt, int &nb) {
+    nb = i % p.nblocks;
+    const int rest = i / p.nblocks;
+    mt = rest % p.tiles_m;
+    b = rest / p.tiles_m;
+  };
+
+  if (warp < 4) {
+    // ------------------------------------------------------------ producers
+    const int m = threadIdx.x;  // pixel within the tile == TMEM lane
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    const int plane_sz = p.TR * p.TC;
+    uint32_t q = 0, hb = 0;
+    for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x) {
+      int b, mt, nb;
+      tile_decode(i, b, mt, nb);
+      const int m0 = mt * kMT;
+      const int pix = m0 + m;
+      const bool valid = pix < npix;
+      const int oy = valid ? pix / g.OW : 0, ox = valid ? pix % g.OW : 0;
+      const int row0 = (m0 / g.OW) * g.down - g.low_r;
+      const int pix_off = (oy * g.down - g.low_r - row0) * p.TC + (ox * g.down - g.low_c - p.start_c);
+      for (int cb = 0; cb < p.NCB && !*abort_flag; ++cb, ++hb) {
+        const int h = hb & 1;
+        if (!mbar_wait(&bars.hfull[h], (hb >> 1) & 1, p.err)) { *abort_flag = 1; break; }
+        const float *halo = reinterpret_cast<const float *>(halo_buf(h));
+        const int cvalid = min(CB, g.n - cb * CB);
+        for (int tap = 0; tap < RS; ++tap, ++q) {
+          const int s = q % kStages;
+          if (!mbar_wait(&bars.empty[s], ((q / kStages) & 1) ^ 1, p.err)) { *abort_flag = 1; break; }
+          const int r = tap / g.S, c = tap - r * g.S;
+          const float *src = halo + pix_off + r * p.TC + c;
+          uint32_t hi[CB / 2], lo[CB / 2];
+#pragma unroll
+          for (int j = 0; j < CB / 2; ++j) {
+            const int c0 = 2 * j, c1 = 2 * j + 1;
+            const float v0 = (valid && c0 < cvalid) ? src[c0 * plane_sz] : 0.0f;
+            const float v1 = (valid && c1 < cvalid) ? src[c1 * plane_sz] : 0.0f;
+            split_bf16x2(v0, v1, hi[j], lo[j]);
+          }
+          const uint32_t acol = tmem + lane_base + a_col0 + (uint32_t)s * CB;
+#pragma unroll
+          for (int j = 0; j < CB / 2; j += 8) {
+            uint32_t h8[8], l8[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+              h8[t] = hi[j + t];
+              l8[t] = lo[j + t];
+            }
+            tmem_st8(acol + j, h8);
+            tmem_st8(acol + CB / 2 + j, l8);
+          }
+          tc_wait_st();
+          tc_fence_before();
+          mbar_arrive(&bars.full[s]);
+        }
+        mbar_arrive(&bars.hempty[h]);
+      }
+    }
+  } else if (warp == kMmaWarp) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(kMT, p.NT);
+      const uint32_t lbo = 128, sbo = CB * 16;
+      const uint32_t img_bytes = (uint32_t)p.NT * CB * 2;
+      uint32_t q = 0, tc = 0;
+      for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x, ++tc) {
+        const int d = tc & 1;
+        if (!mbar_wait(&bars.dempty[d], ((tc >> 1) & 1) ^ 1, p.err)) { *abort_flag = 1; break; }
+        tc_fence_after();
+        const uint32_t dt = tmem + d_col(d);
+        const int nchunks = p.NCB * RS;
+        for (int k = 0; k < nchunks; ++k, ++q) {
+          const int s = q % kStages;
+          if (!mbar_wait(&bars.full[s], (q / kStages) & 1, p.err)) { *abort_flag = 1; break; }
+          tc_fence_after();
+          const uint32_t a_hi = tmem + a_col0 + (uint32_t)s * CB;
+          const uint32_t a_lo = a_hi + CB / 2;
+          const uint32_t b_hi = smem_u32(bstage + (size_t)s * bstage_bytes);
+          const uint32_t b_lo = b_hi + img_bytes;
+#pragma unroll
+          for (int j = 0; j < CB / 16; ++j) {
+            const uint64_t dh = smem_desc_kmajor(b_hi + 256u * j, lbo, sbo);
+            const uint64_t dl = smem_desc_kmajor(b_lo + 256u * j, lbo, sbo);
+            mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc, (k > 0 || j > 0) ? 1u : 0u);
+            mma_bf16_ts(dt, a_hi + 8u * j, dl, idesc, 1u);
+            mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc, 1u);
+          }
+          tc_commit(&bars.empty[s]);
+        }
+        tc_commit(&bars.dfull[d]);
+      }
+    }
+  } else if (warp == kLoadWarp) {
+    // ------------------------------------------------------------ loader
+    if (lane == 0) {
+      const uint32_t halo_tx = (uint32_t)(p.TC * p.TR * CB * 4);
+      // Enumerate (tile, cb) halo blocks in the producers' order.
+      auto halo_issue = [&](uint32_t hbk, int i_tile, int cb) -> bool {
+        const int h = hbk & 1;
+        if (!mbar_wait(&bars.hempty[h], ((hbk >> 1) & 1) ^ 1, p.err)) return false;
+        int b, mt, nb;
+        tile_decode(i_tile, b, mt, nb);
+        const int row0 = ((mt * kMT) / g.OW) * g.down - g.low_r;
+        mbar_arrive_expect_tx(&bars.hfull[h], halo_tx);
+        tma_load_3d(halo_buf(h), &xmap, &bars.hfull[h], p.start_c, row0, b * g.n + cb * CB);
+        return true;
+      };
+      uint32_t q = 0, hb = 0;
+      int next_tile = blockIdx.x, next_cb = 0;
+      bool ok = true;
+      // prefetch the first halo block
+      if (next_tile < p.total_tiles) ok = halo_issue(0, next_tile, 0);
+      for (int i = blockIdx.x; ok && i < p.total_tiles && !*abort_flag; i += gridDim.x) {
+        int b, mt, nb;
+        tile_decode(i, b, mt, nb);
+        for (int cb = 0; ok && cb < p.NCB; ++cb, ++hb) {
+          // prefetch the halo block after this one
+          int ni = i, ncb = cb + 1;
+          if (ncb == p.NCB) { ni = i + gridDim.x; ncb = 0; }
+          if (ni < p.total_tiles) ok = halo_issue(hb + 1, ni, ncb);
+          if (!ok) break;
+          const uint8_t *bsrc = p.bpack + (((size_t)nb * p.NCB + cb) * RS) * bstage_bytes;
+          for (int tap = 0; tap < RS; ++tap, ++q) {
+            const int s = q % kStages;
+            if (!mbar_wait(&bars.empty[s], ((q / kStages) & 1) ^ 1, p.err)) { ok = false; break; }
+            mbar_arrive_expect_tx(&bars.full[s], bstage_bytes);
+            bulk_load(bstage + (size_t)s * bstage_bytes, bsrc + (size_t)tap * bstage_bytes, bstage_bytes,
+                      &bars.full[s]);
+          }
+        }
+      }
+      (void)next_tile;
+      (void)next_cb;
+      if (!ok) *abort_flag = 1;
+      if (*abort_flag) {
+        // Let the copies that may still be in flight land before this CTA's
+        // shared memory is released: the last kStages filter chunks and the
+        // last two halo blocks issued.
+        for (uint32_t qq = q > kStages ? q - kStages : 0; qq < q; ++qq)
+          mbar_wait(&bars.full[qq % kStages], (qq / kStages) & 1, p.err);
+        for (uint32_t hh = hb > 0 ? hb - 1 : 0; hh <= hb + 1; ++hh)
+          mbar_wait(&bars.hfull[hh & 1], (hh >> 1) & 1, p.err);
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int sub = warp & 3;  // TMEM lane quarter this warp may access
+    const int m = sub * 32 + lane;
+    const uint32_t lane_base = (uint32_t)(sub * 32) << 16;
+    const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
+    uint32_t tc = 0;
+    for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x, ++tc) {
+      const int d = tc & 1;
+      if (!mbar_wait(&bars.dfull[d], (tc >> 1) & 1, p.err)) { *abort_flag = 1; break; }
+      tc_fence_after();
+      int b, mt, nb;
+      tile_decode(i, b, mt, nb);
+      const int pix = mt * kMT + m;
+      const bool valid = pix < npix;
+      const int n0 = nb * p.NT;
+      float *ybase = p.y + ((size_t)b * g.groups + n0) * npix + pix;
+      for (int c = 0; c < p.NT; c += 16) {
+        uint32_t v[16];
+        tmem_ld16(tmem + lane_base + d_col(d) + c, v);
+        tc_wait_ld();
+        if (valid) {
+#pragma unroll
+          for (int t = 0; t < 16; ++t) {
+            if (n0 + c + t < g.groups) {
+              float val = __uint_as_float(v[t]);
+              if (relu) val = fmaxf(val, 0.0f);
+              ybase[(size_t)(c + t) * npix] = val;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&bars.dempty[d]);
+    }
+  }
+
+  // ---------------------------------------------------------------- teardown
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kMmaWarp) tmem_dealloc(tmem, 512);
+}
+
+// Pack filters into per-chunk bf16 hi/lo operand images:
+// chunk (nb, cb, tap) = [hi NT x CB][lo NT x CB], row n = output plane
+// nb*NT + n, column ci = input plane cb*CB + ci, value f[plane(n, c)][tap']
+// with tap' flipped for convolution.  Rows/columns past the real counts are 0.
+__global__ void pack_filters_kernel(ConvGeom g, const float *__restrict__ f, uint8_t *__restrict__ out,
+                                    int NT, int CB, int NCB, int nblocks) {
+  const int RS = g.R * g.S;
+  const long long total = (long long)nblocks * NCB * RS * NT * CB;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int ci = (int)(idx % CB);
+    long long rest = idx / CB;
+    const int n = (int)(rest % NT);
+    rest /= NT;
+    const int tap = (int)(rest % RS);
+    rest /= RS;
+    const int cb = (int)(rest % NCB);
+    const int nb = (int)(rest / NCB);
+    const int k = nb * NT + n, c = cb * CB + ci;
+    float v = 0.0f;
+    if (k < g.groups && c < g.n) {
+      // output plane o = k of image 0, term c -> filter plane
+      int ip, fp;
+      plane_pair(g, k, c, &ip, &fp);
+      const int r = tap / g.S, s = tap - r * g.S;
+      const int src = g.orient == CCT_CONVOLUTION ? (g.R - 1 - r) * g.S + (g.S - 1 - s) : tap;
+      v = f[(size_t)fp * RS + src];
+    }
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    const size_t chunk = ((size_t)nb * NCB + cb) * RS + tap;
+    uint8_t *img = out + chunk * (2u * NT * CB * 2);
+    const uint32_t off = packed_offset(n, ci, CB);
+    *reinterpret_cast<__nv_bfloat16 *>(img + off) = h;
+    *reinterpret_cast<__nv_bfloat16 *>(img + NT * CB * 2 + off) = l;
+  }
+}
+
+std::mutex g_tc_mu;
+std::unordered_map<uint64_t, size_t> g_tc_attr;
+
+template <int CB>
+int launch_cb(const TcParams &p0, const float *x, cudaStream_t st) {
+  TcParams p = p0;
+  CUtensorMap map;
+  int rc = encode_tensor_map_3d_box(&map, x, p.g.W, p.g.H, p.g.pin, p.TC, p.TR, CB);
+  if (rc) return rc;
+  const size_t smem = 2 * (size_t)p.halo_bytes + (size_t)kStages * 2u * p.NT * CB * 2;
+  auto kern = frame_tc_kernel<CB>;
+  {
+    // Dynamic shared memory above 48 KB needs the opt-in attribute; keep the
+    // largest size set so far per (device, instance).
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)CB;
+    std::lock_guard<std::mutex> lk(g_tc_mu);
+    size_t &have = g_tc_attr[key];
+    if (have < smem) {
+      rc = check_cuda(cudaFuncSetAttribute((const void *)kern,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                      "cudaFuncSetAttribute(frame_tc)");
+      if (rc) return rc;
+      have = smem;
+    }
+  }
+  kern<<<p.grid, kThreads, smem, st>>>(map, p);
+  count_launches(1);
+  return check_cuda(cudaGetLastError(), "frame_tc_kernel launch");
+}
+
+}  // namespace
+
+// Tile plan for the tensor-core kernel; returns false when the shape is
+// outside what it handles (the FP32 frame kernel takes those).
+bool frame_tc_plan(const ConvGeom &g, int sms, TcParams *out) {
+  if (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM && g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+    return false;
+  if (g.up != 1 || (g.down != 1 && g.down != 2)) return false;
+  if (g.border != CCT_BORDER_ZERO && g.border != CCT_BORDER_FULL && g.border != CCT_BORDER_VALID)
+    return false;
+  if ((g.W & 3) != 0) return false;
+  TcParams p{};
+  p.g = g;
+  const int npix = g.OH * g.OW;
+  p.tiles_m = (npix + kMT - 1) / kMT;
+  p.NT = std::min(128, ((g.groups + 15) / 16) * 16);
+  p.nblocks = (g.groups + p.NT - 1) / p.NT;
+  p.total_tiles = g.batch * p.tiles_m * p.nblocks;
+  // rows of output spanned by any tile
+  int max_rows = 0;
+  for (int mt = 0; mt < p.tiles_m; ++mt) {
+    const int first = (mt * kMT) / g.OW, last = (std::min(npix, (mt + 1) * kMT) - 1) / g.OW;
+    max_rows = std::max(max_rows, last - first + 1);
+  }
+  p.TR = (max_rows - 1) * g.down + g.R;
+  // x origin of the box: -low_c rounded down to a multiple of 4 (TMA rule)
+  const int lc = -g.low_c;
+  p.start_c = lc >= 0 ? (lc / 4) * 4 : -(((-lc) + 3) / 4) * 4;
+  const int off = lc - p.start_c;
+  p.TC = ((off + (g.OW - 1) * g.down + g.S) + 3) & ~3;
+  if (p.TC > 256 || p.TR > 256) return false;
+  const int cmax = ((g.n + 15) / 16) * 16;
+  const size_t budget = 220 * 1024;
+  p.CB = 0;
+  for (int cb : {64, 32, 16}) {
+    if (cb > cmax && cb != 16) continue;
+    const size_t halo = (((size_t)p.TC * p.TR * cb * 4) + 1023) & ~(size_t)1023;
+    const size_t bst = (size_t)kStages * 2u * p.NT * cb * 2;
+    const int tcols = 2 * p.NT + kStages * cb;
+    if (2 * halo + bst <= budget && tcols <= 512) {
+      p.CB = cb;
+      p.halo_bytes = (uint32_t)halo;
+      break;
+    }
+  }
+  if (!p.CB) return false;
+  p.NCB = (g.n + p.CB - 1) / p.CB;
+  p.grid = std::min(p.total_tiles, sms);
+  p.pack_bytes = (size_t)p.nblocks * p.NCB * g.R * g.S * 2u * p.NT * p.CB * 2;
+  *out = p;
+  return true;
+}
+
+int launch_pack_filters(const TcParams &p, const float *f, uint8_t *packed, cudaStream_t st) {
+  const long long total = (long long)p.nblocks * p.NCB * p.g.R * p.g.S * p.NT * p.CB;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  pack_filters_kernel<<<blocks, 256, 0, st>>>(p.g, f, packed, p.NT, p.CB, p.NCB, p.nblocks);
+  count_launches(1);
+  return check_cuda(cudaGetLastError(), "pack_filters_kernel launch");
+}
+
+int launch_frame_tc(const TcParams &p, const float *x, float *y, const uint8_t *packed,
+                    unsigned *err, cudaStream_t st) {
+  TcParams q = p;
+  q.y = y;
+  q.bpack = packed;
+  q.err = err;
+  switch (p.CB) {
+    case 16: return launch_cb<16>(q, x, st);
+    case 32: return launch_cb<32>(q, x, st);
+    case 64: return launch_cb<64>(q, x, st);
+    default: return set_error(CCT_ENOTSUP, "frame_tc: bad channel block %d", p.CB);
+  }
+}
+
+}  // namespace cct

@@ -1,0 +1,136 @@
+"""Tensor-core (split-BF16, FP32 accumulate) frame kernels against the FP64
+oracle.  Tolerance: normwise relative error max|y - ref| / max|ref| <= 1e-5,
+the rel-err bound the path is specified to; RMS error is reported too."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from cctconv import _lib
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _desc(od, precision=_lib.PREC_BF16X3, flags=0):
+    return _lib.new_desc(image_rows=od.rows, image_cols=od.cols, image_planes=od.planes,
+                         filter_rows=od.f_rows, filter_cols=od.f_cols, filter_planes=od.f_planes,
+                         batch_size=od.batch, border=od.border, orientation=od.orient,
+                         sampling=od.sampling, step=od.step, vector_mode=od.mode,
+                         precision=precision, flags=flags)
+
+
+def run_tc(od, x, f, flags=0, expect_tc=True):
+    plan = _lib.Plan(_desc(od, flags=flags))
+    if expect_tc:
+        assert plan.algo == _lib.PLAN_FRAME_BF16X3
+    orows, ocols, oplanes = plan.shape
+    xd = torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+    fd = torch.from_numpy(np.ascontiguousarray(f, np.float32)).cuda()
+    yd = torch.full((oplanes, orows, ocols), float("nan"), device="cuda")
+    plan.run(xd.data_ptr(), fd.data_ptr(), yd.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert _lib.LIB.cct_device_status() == _lib.OK
+    plan.close()
+    return yd.cpu().numpy()
+
+
+def check(y, od, x, f, relu=False):
+    ref = O.conv(od, x, f, np.float64)
+    if relu:
+        ref = np.maximum(ref, 0)
+    assert not np.isnan(y).any()
+    mx, rms = O.rel_errors(y, ref)
+    assert mx <= TOL, (mx, rms)
+    return mx, rms
+
+
+def _cfg2():
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((16 * 32, 64, 64)).astype(np.float32)
+    f = (rng.standard_normal((64 * 32, 5, 5)) * np.sqrt(2.0 / 800)).astype(np.float32)
+    g = rng.standard_normal((16 * 64, 64, 64)).astype(np.float32)
+    return x, f, g
+
+
+def test_config2_project_frame_bf16x3():
+    x, f, _ = _cfg2()
+    od = O.make_desc(64, 64, 5, 5, planes=512, f_planes=2048, batch=16, border=O.ZERO,
+                     orient=O.XCORR, mode=O.PROJECT_REDUCE)
+    mx, rms = check(run_tc(od, x, f), od, x, f)
+    print(f"projectFrame bf16x3: normwise max {mx:.3e} rms {rms:.3e}")
+
+
+def test_config2_back_project_frame_bf16x3():
+    _, f, g = _cfg2()
+    od = O.make_desc(64, 64, 5, 5, planes=1024, f_planes=2048, batch=16, border=O.ZERO,
+                     orient=O.CONV, mode=O.BACKPROJECT_REDUCE)
+    mx, rms = check(run_tc(od, g, f), od, g, f)
+    print(f"backProjectFrame bf16x3: normwise max {mx:.3e} rms {rms:.3e}")
+
+
+TC_CASES = [
+    # (H, W, C, K, B, R, border, sampling, step, mode)
+    (16, 16, 16, 16, 1, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (20, 36, 3, 24, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (28, 28, 64, 48, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (32, 32, 40, 130, 1, 3, O.ZERO, O.DOWN, 2, O.PROJECT_REDUCE),
+    (24, 40, 8, 16, 3, 5, O.VALID, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (12, 20, 8, 16, 2, 5, O.FULL, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (36, 12, 17, 9, 2, 7, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (56, 56, 32, 32, 1, 1, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (16, 16, 32, 16, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
+    (44, 48, 24, 72, 2, 5, O.ZERO, O.DOWN, 2, O.BACKPROJECT_REDUCE),
+]
+
+
+@pytest.mark.parametrize("H,W,C,K,B,R,border,samp,step,mode", TC_CASES)
+def test_tc_shapes(H, W, C, K, B, R, border, samp, step, mode):
+    rng = np.random.default_rng(H * 100 + C * 7 + K)
+    if mode == O.PROJECT_REDUCE:
+        planes, orient = B * C, O.XCORR
+    else:
+        planes, orient = B * K, O.CONV
+    od = O.make_desc(H, W, R, R, planes=planes, f_planes=K * C, batch=B, border=border,
+                     orient=orient, sampling=samp, step=step, mode=mode)
+    x = rng.standard_normal((planes, H, W)).astype(np.float32)
+    f = rng.standard_normal((K * C, R, R)).astype(np.float32)
+    check(run_tc(od, x, f), od, x, f)
+
+
+def test_tc_relu_and_static_filter():
+    rng = np.random.default_rng(77)
+    H, W, C, K, B, R = 32, 32, 16, 32, 2, 3
+    od = O.make_desc(H, W, R, R, planes=B * C, f_planes=K * C, batch=B, border=O.ZERO,
+                     orient=O.XCORR, sampling=O.DOWN, step=2, mode=O.PROJECT_REDUCE)
+    x = rng.standard_normal((B * C, H, W)).astype(np.float32)
+    f = rng.standard_normal((K * C, R, R)).astype(np.float32)
+    check(run_tc(od, x, f, flags=_lib.FLAG_RELU), od, x, f, relu=True)
+    plan = _lib.Plan(_desc(od))
+    plan.set_static_filter(f.ctypes.data)
+    y = np.zeros((B * K, H // 2, W // 2), np.float32)
+    plan.run_host(x.ctypes.data, 0, y.ctypes.data, 0)
+    plan.close()
+    check(y, od, x, f)
+
+
+def test_tc_unsupported_shapes_use_fp32_kernel():
+    # Clamp border is outside the tensor-core path: the plan picks the exact FP32 kernel.
+    od = O.make_desc(16, 16, 3, 3, planes=8, f_planes=16, batch=1, border=O.CLAMP,
+                     orient=O.XCORR, mode=O.PROJECT_REDUCE)
+    plan = _lib.Plan(_desc(od))
+    assert plan.algo == _lib.PLAN_FRAME_F32
+    plan.close()
+
+
+def test_tc_repeatable():
+    """Same inputs, same plan, two runs: identical bits (no races)."""
+    rng = np.random.default_rng(5)
+    od = O.make_desc(64, 64, 5, 5, planes=4 * 32, f_planes=64 * 32, batch=4, border=O.ZERO,
+                     orient=O.XCORR, mode=O.PROJECT_REDUCE)
+    x = rng.standard_normal((128, 64, 64)).astype(np.float32)
+    f = rng.standard_normal((2048, 5, 5)).astype(np.float32)
+    a = run_tc(od, x, f)
+    b = run_tc(od, x, f)
+    assert np.array_equal(a, b)

@@ -9,16 +9,23 @@
 // The reduction walks "chunks": one filter tap x CB input planes.
 //
 // Warp roles (persistent CTAs, one per SM):
-//   warps 0-3  producers: one output pixel per lane; read the CB plane values
-//              of the pixel's tap from the shared-memory halo tile, split
-//              them into bf16 hi/lo and store them to tensor memory as the
-//              A operand (tcgen05.st, row m = lane m).
-//   warp  4    MMA issuer: per chunk 3 x CB/16 tcgen05.mma (A from tensor
-//              memory, B from shared memory) into a double-buffered FP32
-//              accumulator in tensor memory.
-//   warp  5    loader: 3-D TMA loads of the halo tile (zero fill at the
+//   warps 0-15 producers, 4 groups of 4 warps (one warp per tensor-memory
+//              lane quarter, one output pixel per lane).  Together they
+//              split each landed halo block once into bf16 hi/lo; then group
+//              j copies, for every chunk q = j (mod 4), the pixel's split
+//              words of that tap into the chunk's tensor-memory stage
+//              (tcgen05.st, row m = lane m): four chunks are in flight.
+//   warp 16    MMA issuer (one elected lane): per 16-deep k-step of a chunk,
+//              with A from tensor memory and B from shared memory,
+//                NT <= 64: A_hi x [B_hi; B_lo] (N = 2*NT) then A_lo x B_hi
+//                          (N = NT) into the first half: the epilogue adds
+//                          the two halves (a tcgen05.mma costs ~46 cycles
+//                          however narrow, so wide N pays);
+//                NT > 64:  A_hi x B_hi, A_hi x B_lo, A_lo x B_hi (N = NT);
+//              into a double-buffered FP32 accumulator in tensor memory.
+//   warp 17    loader: 3-D TMA loads of the halo tile (zero fill at the
 //              border) and bulk copies of the pre-packed filter chunks.
-//   warps 6-9  epilogue: tcgen05.ld of the accumulator, optional ReLU,
+//   warps 18-21 epilogue: tcgen05.ld of the accumulator, optional ReLU,
 //              coalesced stores to the output planes.
 // Every mbarrier wait is bounded; on a timeout the CTA raises the device
 // error word, lets in-flight copies land, frees its tensor memory and exits.
@@ -37,8 +44,12 @@ namespace {
 
 constexpr int kMT = 128;        // output pixels per tile (MMA M)
 constexpr int kStages = 8;      // A/B chunk pipeline depth
-constexpr int kThreads = 320;   // 10 warps
-constexpr int kMmaWarp = 4, kLoadWarp = 5;  // warps 6-9: epilogue
+constexpr int kGroups = 4;      // producer groups: group j builds chunks q = j (mod kGroups)
+constexpr int kProdWarps = 4 * kGroups;
+constexpr int kProdThreads = 32 * kProdWarps;
+constexpr int kMmaWarp = kProdWarps, kLoadWarp = kProdWarps + 1;  // then 4 epilogue warps
+constexpr int kThreads = 32 * (kProdWarps + 6);
+static_assert(kStages % kGroups == 0, "a stage must always belong to the same producer group");
 
 // Byte offset of element (n, k) inside one packed K-major operand image of
 // rows x CB bf16 (no swizzle): core matrix (8 rows x 8 elements, 128 bytes)
@@ -58,25 +69,34 @@ struct Barriers {
 template <int CB>
 __global__ void __launch_bounds__(kThreads, 1)
     frame_tc_kernel(const __grid_constant__ CUtensorMap xmap, const __grid_constant__ TcParams p) {
+  // Shared memory: [landing: fp32 halo block, planes x TR x TC as TMA writes it]
+  //                [split:   the same block as packed bf16 hi/lo per position]
+  //                [kStages filter-chunk stages]
+  // The split layout holds, per halo position, NCH = CB/4 16-byte chunks:
+  // chunks 0..CB/8-1 = hi words (bf16x2 of planes 2j, 2j+1), then the lo
+  // words.  Chunk k of position pos is stored at chunk slot k ^ (pos % NCH)
+  // so that 8 lanes reading 8 consecutive positions hit distinct banks.
+  constexpr int NCH = CB / 4;
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ Barriers bars;
   const ConvGeom &g = p.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-  auto halo_buf = [&](int h) { return smem + (h ? p.halo_bytes : 0u); };
+  uint8_t *landing = smem;
+  uint8_t *split = smem + p.halo_bytes;
   uint8_t *bstage = smem + 2 * p.halo_bytes;
   const uint32_t bstage_bytes = 2u * p.NT * CB * 2;  // hi + lo images
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
-      mbar_init(&bars.full[s], 129);  // 128 producer arrivals + loader expect_tx
+      mbar_init(&bars.full[s], 5);    // the 4 warps of the chunk's group + loader expect_tx
       mbar_init(&bars.empty[s], 1);   // MMA commit
     }
+    mbar_init(&bars.hfull[0], 1);     // halo block landed (TMA)
+    mbar_init(&bars.hempty[0], kProdWarps);  // halo block converted (one arrival per producer warp)
     for (int h = 0; h < 2; ++h) {
-      mbar_init(&bars.hfull[h], 1);
-      mbar_init(&bars.hempty[h], 128);
       mbar_init(&bars.dfull[h], 1);
-      mbar_init(&bars.dempty[h], 128);
+      mbar_init(&bars.dempty[h], 4);  // one arrival per epilogue warp
     }
     bars.abort_flag = 0;
     fence_barrier_init();
@@ -89,8 +109,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int RS = g.R * g.S;
   const int npix = g.OH * g.OW;
-  auto d_col = [&](int d) { return d ? (uint32_t)p.NT : 0u; };
-  const uint32_t a_col0 = 2u * p.NT;  // stage s: hi at a_col0 + s*CB, lo at + CB/2
+  const bool concat = p.NT <= 64;                 // [B_hi; B_lo] in one MMA
+  const uint32_t dw = concat ? 2u * p.NT : (uint32_t)p.NT;  // accumulator width
+  auto d_col = [&](int d) { return d ? dw : 0u; };
+  const uint32_t a_col0 = 2u * dw;  // stage s: hi at a_col0 + s*CB, lo at + CB/2
   volatile int *abort_flag = &bars.abort_flag;
 
   auto tile_decode = [&](int i, int &b, int &mt, int &nb) {
@@ -100,13 +122,19 @@ __global__ void __launch_bounds__(kThreads, 1)
     b = rest / p.tiles_m;
   };
 
-  if (warp < 4) {
+  if (warp < kProdWarps) {
     // ------------------------------------------------------------ producers
-    const int m = threadIdx.x;  // pixel within the tile == TMEM lane
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    const int plane_sz = p.TR * p.TC;
+    const int quarter = warp & 3, group = warp >> 2;
+    const int m = quarter * 32 + lane;  // pixel within the tile == TMEM lane
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    const int npos = p.TR * p.TC;
+    const float *land = reinterpret_cast<const float *>(landing);
+    uint4 *spl = reinterpret_cast<uint4 *>(split);
+    // The exit decision is taken jointly at the group's named barriers
+    // (bar.red.or), so no producer can leave while the others wait there.
     uint32_t q = 0, hb = 0;
-    for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x) {
+    bool failed = false;
+    for (int i = blockIdx.x; i < p.total_tiles; i += gridDim.x) {
       int b, mt, nb;
       tile_decode(i, b, mt, nb);
       const int m0 = mt * kMT;
@@ -114,107 +142,156 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool valid = pix < npix;
       const int oy = valid ? pix / g.OW : 0, ox = valid ? pix % g.OW : 0;
       const int row0 = (m0 / g.OW) * g.down - g.low_r;
-      const int pix_off = (oy * g.down - g.low_r - row0) * p.TC + (ox * g.down - g.low_c - p.start_c);
-      for (int cb = 0; cb < p.NCB && !*abort_flag; ++cb, ++hb) {
-        const int h = hb & 1;
-        if (!mbar_wait(&bars.hfull[h], (hb >> 1) & 1, p.err)) { *abort_flag = 1; break; }
-        const float *halo = reinterpret_cast<const float *>(halo_buf(h));
+      const int pos0 = (oy * g.down - g.low_r - row0) * p.TC + (ox * g.down - g.low_c - p.start_c);
+      for (int cb = 0; cb < p.NCB; ++cb, ++hb) {
+        // 1. all producers convert the landed fp32 block into split bf16 hi/lo
+        failed = named_sync_or(1, kProdThreads, failed || *abort_flag);  // previous block fully read
+        if (failed) break;
+        if (!mbar_wait(&bars.hfull[0], hb & 1, p.err)) failed = true;
         const int cvalid = min(CB, g.n - cb * CB);
-        for (int tap = 0; tap < RS; ++tap, ++q) {
-          const int s = q % kStages;
-          if (!mbar_wait(&bars.empty[s], ((q / kStages) & 1) ^ 1, p.err)) { *abort_flag = 1; break; }
-          const int r = tap / g.S, c = tap - r * g.S;
-          const float *src = halo + pix_off + r * p.TC + c;
-          uint32_t hi[CB / 2], lo[CB / 2];
+        for (int pos = threadIdx.x; !failed && pos < npos; pos += kProdThreads) {
+          uint4 *dst = spl + (size_t)pos * NCH;
+          const int sw = pos % NCH;
 #pragma unroll
-          for (int j = 0; j < CB / 2; ++j) {
-            const int c0 = 2 * j, c1 = 2 * j + 1;
-            const float v0 = (valid && c0 < cvalid) ? src[c0 * plane_sz] : 0.0f;
-            const float v1 = (valid && c1 < cvalid) ? src[c1 * plane_sz] : 0.0f;
-            split_bf16x2(v0, v1, hi[j], lo[j]);
-          }
-          const uint32_t acol = tmem + lane_base + a_col0 + (uint32_t)s * CB;
+          for (int k = 0; k < CB / 8; ++k) {  // 8 planes -> one hi and one lo chunk
+            uint32_t hi[4], lo[4];
 #pragma unroll
-          for (int j = 0; j < CB / 2; j += 8) {
-            uint32_t h8[8], l8[8];
-#pragma unroll
-            for (int t = 0; t < 8; ++t) {
-              h8[t] = hi[j + t];
-              l8[t] = lo[j + t];
+            for (int j = 0; j < 4; ++j) {
+              const int c0 = 8 * k + 2 * j;
+              const float v0 = (c0 < cvalid) ? land[c0 * npos + pos] : 0.0f;
+              const float v1 = (c0 + 1 < cvalid) ? land[(c0 + 1) * npos + pos] : 0.0f;
+              split_bf16x2(v0, v1, hi[j], lo[j]);
             }
-            tmem_st8(acol + j, h8);
-            tmem_st8(acol + CB / 2 + j, l8);
+            dst[k ^ sw] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            dst[(k + CB / 8) ^ sw] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
           }
-          tc_wait_st();
-          tc_fence_before();
-          mbar_arrive(&bars.full[s]);
         }
-        mbar_arrive(&bars.hempty[h]);
+        failed = named_sync_or(1, kProdThreads, failed);  // the split block is complete
+        if (failed) break;
+        if (lane == 0) mbar_arrive(&bars.hempty[0]);  // the landing buffer may be refilled
+        // 2. this group's chunks: copy the pixel's split words of the tap to TMEM
+        int r = 0, c = 0;
+        for (int tap = 0; tap < RS; ++tap, ++q) {
+          if ((int)(q % kGroups) == group) {
+            const int s = q % kStages;
+            bool bad = failed || *abort_flag;
+            if (!bad) bad = !mbar_wait(&bars.empty[s], ((q / kStages) & 1) ^ 1, p.err);
+            if (__any_sync(0xffffffffu, bad)) {  // warp-uniform: tcgen05.st is warp-collective
+              failed = true;
+            } else {
+              tc_fence_after();
+              const int pos = pos0 + r * p.TC + c;
+              const uint4 *src = spl + (size_t)pos * NCH;
+              const int sw = pos % NCH;
+              const uint32_t acol = tmem + lane_base + a_col0 + (uint32_t)s * CB;
+#pragma unroll
+              for (int k = 0; k < NCH; k += 2) {
+                const uint4 w0 = valid ? src[k ^ sw] : make_uint4(0, 0, 0, 0);
+                const uint4 w1 = valid ? src[(k + 1) ^ sw] : make_uint4(0, 0, 0, 0);
+                const uint32_t v8[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+                tmem_st8(acol + 4 * k, v8);  // hi words fill columns [0, CB/2), lo words [CB/2, CB)
+              }
+              tc_wait_st();
+              tc_fence_before();
+              __syncwarp();
+              if (lane == 0) mbar_arrive(&bars.full[s]);
+            }
+          }
+          if (++c == g.S) {
+            c = 0;
+            ++r;
+          }
+        }
       }
+      if (failed) break;
     }
+    if (failed) *abort_flag = 1;
   } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
-    if (lane == 0) {
-      const uint32_t idesc = idesc_bf16_f32(kMT, p.NT);
-      const uint32_t lbo = 128, sbo = CB * 16;
-      const uint32_t img_bytes = (uint32_t)p.NT * CB * 2;
-      uint32_t q = 0, tc = 0;
-      for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x, ++tc) {
-        const int d = tc & 1;
-        if (!mbar_wait(&bars.dempty[d], ((tc >> 1) & 1) ^ 1, p.err)) { *abort_flag = 1; break; }
+    // The whole warp walks the loop (its values stay warp-uniform); one
+    // elected lane issues the tcgen05 instructions.
+    const uint32_t idesc_n = idesc_bf16_f32(kMT, p.NT);
+    const uint32_t idesc_2n = idesc_bf16_f32(kMT, 2 * p.NT);
+    const uint32_t lbo = 128, sbo = CB * 16;
+    const uint32_t img_bytes = (uint32_t)p.NT * CB * 2;
+    const uint32_t bstage0 = smem_u32(bstage);
+    uint32_t q = 0, tc = 0;
+    bool failed = false;
+    for (int i = blockIdx.x; i < p.total_tiles; i += gridDim.x, ++tc) {
+      const int d = tc & 1;
+      failed = __any_sync(0xffffffffu, failed || *abort_flag ||
+                                           !mbar_wait(&bars.dempty[d], ((tc >> 1) & 1) ^ 1, p.err));
+      if (failed) break;
+      tc_fence_after();
+      const uint32_t dt = tmem + d_col(d);
+      const int nchunks = p.NCB * RS;
+      for (int k = 0; k < nchunks; ++k, ++q) {
+        const int s = q % kStages;
+        failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[s], (q / kStages) & 1, p.err));
+        if (failed) break;
         tc_fence_after();
-        const uint32_t dt = tmem + d_col(d);
-        const int nchunks = p.NCB * RS;
-        for (int k = 0; k < nchunks; ++k, ++q) {
-          const int s = q % kStages;
-          if (!mbar_wait(&bars.full[s], (q / kStages) & 1, p.err)) { *abort_flag = 1; break; }
-          tc_fence_after();
-          const uint32_t a_hi = tmem + a_col0 + (uint32_t)s * CB;
-          const uint32_t a_lo = a_hi + CB / 2;
-          const uint32_t b_hi = smem_u32(bstage + (size_t)s * bstage_bytes);
-          const uint32_t b_lo = b_hi + img_bytes;
+        const uint32_t a_hi = tmem + a_col0 + (uint32_t)s * CB;
+        const uint32_t a_lo = a_hi + CB / 2;
+        const uint32_t b_hi = bstage0 + (uint32_t)s * bstage_bytes;
+        const uint32_t b_lo = b_hi + img_bytes;
+        if (elect_one()) {
 #pragma unroll
           for (int j = 0; j < CB / 16; ++j) {
+            const uint32_t acc = (k > 0 || j > 0) ? 1u : 0u;
             const uint64_t dh = smem_desc_kmajor(b_hi + 256u * j, lbo, sbo);
-            const uint64_t dl = smem_desc_kmajor(b_lo + 256u * j, lbo, sbo);
-            mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc, (k > 0 || j > 0) ? 1u : 0u);
-            mma_bf16_ts(dt, a_hi + 8u * j, dl, idesc, 1u);
-            mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc, 1u);
+            if (concat) {
+              mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_2n, acc);  // [hi*hi | hi*lo]
+              mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc_n, 1u);    // + lo*hi
+            } else {
+              const uint64_t dl = smem_desc_kmajor(b_lo + 256u * j, lbo, sbo);
+              mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_n, acc);
+              mma_bf16_ts(dt, a_hi + 8u * j, dl, idesc_n, 1u);
+              mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc_n, 1u);
+            }
           }
           tc_commit(&bars.empty[s]);
         }
-        tc_commit(&bars.dfull[d]);
+        __syncwarp();
       }
+      if (failed) break;
+      if (elect_one()) tc_commit(&bars.dfull[d]);
+      __syncwarp();
     }
+    if (failed) *abort_flag = 1;
   } else if (warp == kLoadWarp) {
     // ------------------------------------------------------------ loader
     if (lane == 0) {
       const uint32_t halo_tx = (uint32_t)(p.TC * p.TR * CB * 4);
-      // Enumerate (tile, cb) halo blocks in the producers' order.
-      auto halo_issue = [&](uint32_t hbk, int i_tile, int cb) -> bool {
-        const int h = hbk & 1;
-        if (!mbar_wait(&bars.hempty[h], ((hbk >> 1) & 1) ^ 1, p.err)) return false;
+      // Halo blocks in the producers' order: (tile, cb) for this CTA's tiles.
+      int h_tile = blockIdx.x, h_cb = 0;  // next halo block to issue
+      uint32_t h_issued = 0;
+      auto halo_ready_to_issue = [&](bool block) -> int {
+        // 1 issued, 0 not yet possible, -1 timed out
+        if (h_tile >= p.total_tiles) return 0;
+        const uint32_t parity = (h_issued & 1) ^ 1;
+        if (block) {
+          if (!mbar_wait(&bars.hempty[0], parity, p.err)) return -1;
+        } else if (!mbar_test(&bars.hempty[0], parity)) {
+          return 0;
+        }
         int b, mt, nb;
-        tile_decode(i_tile, b, mt, nb);
+        tile_decode(h_tile, b, mt, nb);
         const int row0 = ((mt * kMT) / g.OW) * g.down - g.low_r;
-        mbar_arrive_expect_tx(&bars.hfull[h], halo_tx);
-        tma_load_3d(halo_buf(h), &xmap, &bars.hfull[h], p.start_c, row0, b * g.n + cb * CB);
-        return true;
+        mbar_arrive_expect_tx(&bars.hfull[0], halo_tx);
+        tma_load_3d(landing, &xmap, &bars.hfull[0], p.start_c, row0, b * g.n + h_cb * CB);
+        ++h_issued;
+        if (++h_cb == p.NCB) {
+          h_cb = 0;
+          h_tile += gridDim.x;
+        }
+        return 1;
       };
+      bool ok = halo_ready_to_issue(true) >= 0;
       uint32_t q = 0, hb = 0;
-      int next_tile = blockIdx.x, next_cb = 0;
-      bool ok = true;
-      // prefetch the first halo block
-      if (next_tile < p.total_tiles) ok = halo_issue(0, next_tile, 0);
       for (int i = blockIdx.x; ok && i < p.total_tiles && !*abort_flag; i += gridDim.x) {
         int b, mt, nb;
         tile_decode(i, b, mt, nb);
         for (int cb = 0; ok && cb < p.NCB; ++cb, ++hb) {
-          // prefetch the halo block after this one
-          int ni = i, ncb = cb + 1;
-          if (ncb == p.NCB) { ni = i + gridDim.x; ncb = 0; }
-          if (ni < p.total_tiles) ok = halo_issue(hb + 1, ni, ncb);
-          if (!ok) break;
           const uint8_t *bsrc = p.bpack + (((size_t)nb * p.NCB + cb) * RS) * bstage_bytes;
           for (int tap = 0; tap < RS; ++tap, ++q) {
             const int s = q % kStages;
@@ -222,20 +299,21 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_arrive_expect_tx(&bars.full[s], bstage_bytes);
             bulk_load(bstage + (size_t)s * bstage_bytes, bsrc + (size_t)tap * bstage_bytes, bstage_bytes,
                       &bars.full[s]);
+            // prefetch the next halo block as soon as the landing buffer is free
+            if (h_issued == hb + 1 && halo_ready_to_issue(false) < 0) ok = false;
           }
+          // the producers need the next block before they can go on
+          if (ok && h_issued == hb + 1 && halo_ready_to_issue(true) < 0) ok = false;
         }
       }
-      (void)next_tile;
-      (void)next_cb;
       if (!ok) *abort_flag = 1;
       if (*abort_flag) {
-        // Let the copies that may still be in flight land before this CTA's
+        // Let copies that may still be in flight land before this CTA's
         // shared memory is released: the last kStages filter chunks and the
-        // last two halo blocks issued.
+        // last halo block issued.
         for (uint32_t qq = q > kStages ? q - kStages : 0; qq < q; ++qq)
           mbar_wait(&bars.full[qq % kStages], (qq / kStages) & 1, p.err);
-        for (uint32_t hh = hb > 0 ? hb - 1 : 0; hh <= hb + 1; ++hh)
-          mbar_wait(&bars.hfull[hh & 1], (hh >> 1) & 1, p.err);
+        if (h_issued > 0) mbar_wait(&bars.hfull[0], (h_issued - 1) & 1, p.err);
       }
     }
   } else {
@@ -245,9 +323,14 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t lane_base = (uint32_t)(sub * 32) << 16;
     const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
     uint32_t tc = 0;
-    for (int i = blockIdx.x; i < p.total_tiles && !*abort_flag; i += gridDim.x, ++tc) {
+    for (int i = blockIdx.x; i < p.total_tiles; i += gridDim.x, ++tc) {
+      if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
       const int d = tc & 1;
-      if (!mbar_wait(&bars.dfull[d], (tc >> 1) & 1, p.err)) { *abort_flag = 1; break; }
+      const bool bad = !mbar_wait(&bars.dfull[d], (tc >> 1) & 1, p.err);
+      if (__any_sync(0xffffffffu, bad)) {  // warp-uniform: tcgen05.ld is warp-collective
+        *abort_flag = 1;
+        break;
+      }
       tc_fence_after();
       int b, mt, nb;
       tile_decode(i, b, mt, nb);
@@ -256,14 +339,16 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int n0 = nb * p.NT;
       float *ybase = p.y + ((size_t)b * g.groups + n0) * npix + pix;
       for (int c = 0; c < p.NT; c += 16) {
-        uint32_t v[16];
+        uint32_t v[16], v2[16];
         tmem_ld16(tmem + lane_base + d_col(d) + c, v);
+        if (concat) tmem_ld16(tmem + lane_base + d_col(d) + p.NT + c, v2);
         tc_wait_ld();
         if (valid) {
 #pragma unroll
           for (int t = 0; t < 16; ++t) {
             if (n0 + c + t < g.groups) {
               float val = __uint_as_float(v[t]);
+              if (concat) val += __uint_as_float(v2[t]);
               if (relu) val = fmaxf(val, 0.0f);
               ybase[(size_t)(c + t) * npix] = val;
             }
@@ -271,7 +356,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       tc_fence_before();
-      mbar_arrive(&bars.dempty[d]);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars.dempty[d]);
     }
   }
 
@@ -390,7 +476,8 @@ bool frame_tc_plan(const ConvGeom &g, int sms, TcParams *out) {
     if (cb > cmax && cb != 16) continue;
     const size_t halo = (((size_t)p.TC * p.TR * cb * 4) + 1023) & ~(size_t)1023;
     const size_t bst = (size_t)kStages * 2u * p.NT * cb * 2;
-    const int tcols = 2 * p.NT + kStages * cb;
+    const int dw = p.NT <= 64 ? 2 * p.NT : p.NT;
+    const int tcols = 2 * dw + kStages * cb;
     if (2 * halo + bst <= budget && tcols <= 512) {
       p.CB = cb;
       p.halo_bytes = (uint32_t)halo;

@@ -49,7 +49,12 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 
 // Returns true when the phase with the given parity has completed; false if
 // the poll budget ran out (the error word is set).
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity);
+
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned *err) {
+  // Fast path: a non-blocking probe; try_wait (which may suspend the thread)
+  // only when the phase is still open.
+  if (mbar_test(bar, parity)) return true;
   const uint32_t addr = smem_u32(bar);
   for (uint32_t i = 0; i < kMaxWaitPolls; ++i) {
     uint32_t done;
@@ -63,6 +68,31 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsign
   }
   atomicOr(err, kErrWaitTimeout);
   return false;
+}
+
+// Non-blocking probe: has the phase with this parity completed?
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// Named barrier over `count` threads (ids 1..15; 0 is __syncthreads) that
+// also ORs a predicate across them: every participant gets the same answer.
+__device__ __forceinline__ bool named_sync_or(int id, int count, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n"
+      " selp.u32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(id), "r"(count)
+      : "memory");
+  return r != 0;
 }
 
 // 3-D tiled TMA load (x innermost) into shared memory, completing on `bar`.
@@ -87,6 +117,15 @@ int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols,
 namespace cct {
 
 // ---- tcgen05 (5th-generation tensor core, tensor memory) ------------------
+
+// One lane of the (fully converged) warp returns true.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t pred = 0;
+  asm volatile(
+      "{\n .reg .b32 r;\n .reg .pred p;\n elect.sync r|p, 0xffffffff;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(pred));
+  return pred != 0;
+}
 
 // Allocate / free tensor-memory columns (whole warp, .sync.aligned).
 __device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols) {

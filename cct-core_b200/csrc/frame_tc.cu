@@ -62,6 +62,7 @@ struct Barriers {
   uint64_t full[kStages], empty[kStages];
   uint64_t hfull[2], hempty[2];
   uint64_t dfull[2], dempty[2];
+  uint64_t drain;  // MMA warp: all issued MMAs retired
   uint32_t tmem_slot;
   int abort_flag;
 };
@@ -98,6 +99,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&bars.dfull[h], 1);
       mbar_init(&bars.dempty[h], 4);  // one arrival per epilogue warp
     }
+    mbar_init(&bars.drain, 1);
     bars.abort_flag = 0;
     fence_barrier_init();
   }
@@ -258,6 +260,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncwarp();
     }
     if (failed) *abort_flag = 1;
+    // Every MMA issued has retired before tensor memory can be released.
+    if (elect_one()) tc_commit(&bars.drain);
+    __syncwarp();
+    mbar_wait(&bars.drain, 0, p.err);
   } else if (warp == kLoadWarp) {
     // ------------------------------------------------------------ loader
     if (lane == 0) {

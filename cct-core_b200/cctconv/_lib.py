@@ -70,6 +70,7 @@ SIGNATURES = {
     "cct_conv_run": (_I, [_P, _P, _P, _P, _P]),
     "cct_conv_run_host": (_I, [_P, _P, _P, _P, _P]),
     "cct_conv_separable": (_I, [_I32, _I32, _I32, _P, _P, _I32, _P, _I32, _I32, _I32, _P, _P, _P]),
+    "cct_conv_run_noalloc": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P]),
     "cct_malloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
     "cct_free": (_I, [_P]),
     "cct_memcpy_h2d": (_I, [_P, _P, ctypes.c_size_t, _P]),

@@ -161,6 +161,8 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
   return CCT_OK;
 }
 
+int resolve_geom(const cct_conv_desc *desc, ConvGeom *g) { return resolve(desc, g); }
+
 }  // namespace cct
 
 using namespace cct;

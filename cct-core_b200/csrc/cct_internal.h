@@ -67,6 +67,10 @@ __host__ __device__ inline void plane_pair(const ConvGeom &g, int o, int t,
   }
 }
 
+// Validate a descriptor and resolve its geometry (the rules of
+// cct_conv_output_shape).  Returns CCT_OK or CCT_EINVAL.
+int resolve_geom(const cct_conv_desc *desc, ConvGeom *g);
+
 // Error reporting (thread-local message, returned status).
 int set_error(int status, const char *fmt, ...);
 int check_cuda(cudaError_t e, const char *what);

@@ -149,6 +149,24 @@ int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes,
                        int32_t col_len, int32_t border, int32_t orientation,
                        float *tmp, float *out, void *stream);
 
+/* Allocation-free variant of the BF16X3 BlockReduceSum frame convolution (no
+ * counterpart in the reference, which always lets its runtime own device
+ * buffers).  For callers that cannot call cudaMalloc when they convolve:
+ * hosts that reserve all device memory up front in their own arena, and
+ * latency-sensitive callers for whom cudaMalloc/cudaFree (which may
+ * synchronise the device) are off limits.  It creates no plan and allocates
+ * nothing: image, filter and out are the caller's device pointers; the
+ * kernel's only scratch, the packed bf16 hi/lo filter operand, lives in a
+ * fixed device array of 4 MiB (held by every GPU that loads the library
+ * until exit).  Descriptors whose packed operand exceeds 4 MiB are rejected
+ * with CCT_EINVAL; shapes the tensor-core kernel does not take return
+ * CCT_ENOTSUP.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls on a device share the array: calls that overlap on
+ * the GPU race and must be ordered by the caller. */
+int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *image,
+                         const float *filter, float *out, void *stream);
+
 /* ---- device memory helpers (the JNI side has no CUDA runtime) ----------- */
 int cct_malloc(void **ptr, size_t bytes);
 int cct_free(void *ptr);

@@ -255,21 +255,24 @@ def time_steps(fn, steps, warmup, pg):
     return start.elapsed_time(end) / 1e3, _lib.launch_count() - n0
 
 
-def time_single_launch(fn, reps=20):
-    """Average duration of one launch of the dominant kernel (CUDA events on
-    the launching stream)."""
+def time_single_launch(fn, reps=20, rounds=5):
+    """Average device time of one launch of the dominant kernel: `reps`
+    launches back to back between two CUDA events on the launching stream
+    (so host-side launch latency is not counted), median over rounds."""
     import torch
     for _ in range(3):
         fn()
     torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(reps)]
-    for a, b in evs:
+    times = []
+    for _ in range(rounds):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        fn()
+        for _ in range(reps):
+            fn()
         b.record()
-    torch.cuda.synchronize()
-    return statistics.mean(a.elapsed_time(b) for a, b in evs) / 1e3
+        b.synchronize()
+        times.append(a.elapsed_time(b) / 1e3 / reps)
+    return statistics.median(times)
 
 
 def load_peaks():

@@ -9,7 +9,12 @@ He-normal (std sqrt(2/800)); g: 64x64 of 16*64 planes ~ N(0,1).
 2 x 6.711 GFLOP per step (2*B*H*W*K*C*R*S each way).
 
 Other workloads (--workload): plain (256x256 (*) 5x5, BorderZero, batched
-over 4096 planes for the HBM roofline), separable.
+over 4096 planes for the HBM roofline); fft (2048x2048 uniform[0,1] (*) 63x63
+normalised Gaussian, sigma 10, BorderCyclic, through the FFT path, with its
+max/RMS error against an FP64 FFT and the direct kernel's time beside it);
+graph (the eight-layer 3x3 stack on 224x224x3, widths 64..512, stepped as
+one captured launch sequence; batch 64 headline, batches 1 and 8 and FP32
+beside it).
 
 Prints one JSON line (rank 0).  Multi-GPU: replicas only -- every rank runs
 the same step on its own GPU; value = all ranks' work / max rank time.
@@ -35,7 +40,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["frame", "plain", "separable"], default="frame")
+    ap.add_argument("--workload", choices=["frame", "plain", "fft", "graph"], default="frame")
     ap.add_argument("--precision", choices=["auto", "fp32", "bf16x3"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -236,6 +241,185 @@ def plain_workload():
     }
 
 
+def gaussian_filter(k=63, sigma=10.0):
+    import numpy as np
+    r = np.arange(k) - k // 2
+    g = np.exp(-(r[:, None] ** 2 + r[None, :] ** 2) / (2 * sigma * sigma))
+    return (g / g.sum()).astype(np.float32)
+
+
+def fft_workload():
+    """2048x2048 uniform[0,1] ScalarField (*) 63x63 normalised Gaussian,
+    BorderCyclic.  The Gaussian is a constant filter, so its spectrum is made
+    once on the host in FP64 (static filter), as the reference does for
+    constant filters; each step transforms one image and inverts."""
+    import numpy as np
+    import torch
+    import cctconv as C
+    from cctconv import _lib
+
+    n, k = 2048, 63
+    f_host = gaussian_filter(k)
+    mk = lambda algo: _lib.Plan(C.make_desc((n, n, 0), (k, k, 0), C.BorderCyclic,  # noqa: E731
+                                            _lib.CONVOLUTION, C.NoSamplingConvolution,
+                                            _lib.PLANE_BY_PLANE, algo=algo))
+    plan = mk(_lib.ALGO_FFT)
+    plan.set_static_filter(f_host.ctypes.data)
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    sets = 8  # 8 x 33.5 MB of images and outputs > 126 MB L2
+    xs = [torch.empty((n, n), device="cuda").uniform_(0, 1, generator=gen) for _ in range(sets)]
+    ys = [torch.empty((n, n), device="cuda") for _ in range(sets)]
+    stream = torch.cuda.current_stream().cuda_stream
+    state = {"i": 0}
+
+    def step():
+        i = state["i"] % sets
+        state["i"] += 1
+        plan.run(xs[i].data_ptr(), 0, ys[i].data_ptr(), stream)
+
+    # error of the FFT path against an FP64 FFT of the same cyclic convolution
+    step()
+    torch.cuda.synchronize()
+    x64 = xs[0].double().cpu().numpy()
+    g = np.zeros((n, n))
+    h = k // 2
+    for r in range(k):
+        for s in range(k):
+            g[(r - h) % n, (s - h) % n] += f_host[r, s]
+    ref = np.real(np.fft.ifft2(np.fft.fft2(x64) * np.fft.fft2(g)))
+    d = ys[0].double().cpu().numpy() - ref
+    err = {"max_rel": float(np.abs(d).max() / np.abs(ref).max()),
+           "rms_rel": float(np.sqrt((d * d).mean() / (ref * ref).mean()))}
+
+    # the direct kernel on the same convolution, beside it
+    direct = mk(_lib.ALGO_DIRECT)
+    fd = torch.from_numpy(f_host).cuda()
+    yd = torch.empty((n, n), device="cuda")
+    direct_s = time_single_launch(lambda: direct.run(xs[0].data_ptr(), fd.data_ptr(),
+                                                     yd.data_ptr(), stream), reps=3, rounds=3)
+    torch.cuda.synchronize()
+    dd = yd.double().cpu().numpy() - ref
+    err["direct_max_rel"] = float(np.abs(dd).max() / np.abs(ref).max())
+    # dynamic filter: the filter spectrum is made on the device every run
+    dyn = mk(_lib.ALGO_FFT)
+    dyn_s = time_single_launch(lambda: dyn.run(xs[0].data_ptr(), fd.data_ptr(), yd.data_ptr(),
+                                               stream))
+
+    hx = xs[0].cpu().pin_memory()
+    hy = torch.empty((n, n)).pin_memory()
+
+    def e2e_step():
+        plan.run_host(hx.data_ptr(), 0, hy.data_ptr(), stream)
+
+    gflop = 2.0 * n * n * k * k / 1e9  # direct-equivalent work of one convolution
+    return {
+        "step": step, "e2e_step": e2e_step, "launch_single": step,
+        "gflop_per_step": gflop, "gflop_per_launch": gflop,
+        # HBM bytes a run must move: the image in, the filter spectrum in, the result out
+        "bytes_per_step": 4 * n * n * 2 + 8 * n * (n // 2 + 1),
+        "bytes_per_launch": 4 * n * n * 2 + 8 * n * (n // 2 + 1),
+        "e2e_gb_per_step": None, "h2d": 4 * n * n, "d2h": 4 * n * n,
+        "metric": "GFLOP/s", "unit": "GFLOP/s", "precision": "fp32", "plan_algo": plan.algo,
+        "config": {"workload": "FFT convolve 2048x2048 uniform[0,1] (*) 63x63 normalised Gaussian "
+                               "(sigma 10), BorderCyclic, static filter",
+                   "H": n, "W": n, "R": k, "border": "BorderCyclic",
+                   "flops": "direct-equivalent 2*H*W*R*S per convolution",
+                   "l2": "8 rotating image/output sets (268 MB > 126 MB L2)"},
+        "dtype": "f32", "keep": (plan, direct, dyn, xs, ys, fd, yd, hx, hy),
+        "kernel": "fft_rows_r2c+fft_cols+fft_rows_c2r", "fft_hbm_roofline": True,
+        "extra": {"error_vs_fp64": err, "direct_ms": round(direct_s * 1e3, 4),
+                  "dynamic_filter_ms": round(dyn_s * 1e3, 4)},
+    }
+
+
+def graph_workload(precision):
+    """The eight-layer stack (224x224x3 input, 3x3 filters, widths 64, 64,
+    128, 128, 256, 256, 512, 512, DownsampleOutput(2) on layers 2, 4 and 6,
+    ReLU between layers) stepped as a ComputeGraph: each step one replay of
+    the captured launches.  Inputs uniform[-1,1], He-normal filters."""
+    import numpy as np
+    import torch
+    from cctconv import _lib
+    from cctconv.graph import eight_layer_stack
+
+    prec = _lib.PREC_FP32 if precision == "fp32" else _lib.PREC_BF16X3
+
+    def build(batch, p):
+        st = eight_layer_stack(batch, p)
+        rng = np.random.default_rng(4)
+        fs = []
+        for i, (kc, r, s_) in enumerate(st.filter_shapes):
+            c = kc // (st.field_shapes[i + 1][0] // batch)
+            fs.append((rng.standard_normal((kc, r, s_)) * np.sqrt(2.0 / (c * r * s_))).astype(np.float32))
+        st.set_filters(fs)
+        st.input.uniform_(-1, 1)
+        return st
+
+    B = 64
+    stack = build(B, prec)
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        stack.step(1, stream)
+
+    def side(batch, p, steps=20):
+        st = stack if (batch == B and p == prec) else build(batch, p)
+        st.step(3, stream)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        st.step(steps, stream)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b) / steps
+        out = {"ms_per_step": round(ms, 4), "GFLOP/s": round(st.flops_per_step / ms / 1e6, 1)}
+        if st is not stack:
+            st.close()
+        return out
+
+    extra = {"by_batch": {}}
+    for p_name, p in (("bf16x3", _lib.PREC_BF16X3), ("fp32", _lib.PREC_FP32)):
+        for b in (1, 8, 64):
+            extra["by_batch"][f"{p_name}_b{b}"] = side(b, p)
+
+    hx = stack.input.cpu().pin_memory()
+    hy = torch.empty(stack.field_shapes[-1]).pin_memory()
+
+    def e2e_step():
+        stack.step_host(hx, hy, stream)
+
+    gflop = stack.flops_per_step / 1e9
+    # the dominant kernel: layer 8 (28x28, 512 -> 512), timed alone on its plan
+    last = _lib.Plan(stack.descs[-1])
+    lin = stack.field(len(stack.descs) - 1)
+    lf = torch.randn(stack.filter_shapes[-1], device="cuda") * 0.02
+    ly = torch.empty(stack.field_shapes[-1], device="cuda")
+    if last.algo == _lib.PLAN_FRAME_BF16X3:
+        last.set_static_filter(lf.cpu().numpy().ctypes.data)
+        lf_ptr = 0
+    else:
+        lf_ptr = lf.data_ptr()
+    d = stack.descs[-1]
+    last_gflop = 2.0 * B * 512 * 28 * 28 * 512 * 9 / 1e9
+    return {
+        "step": step, "e2e_step": e2e_step,
+        "launch_single": lambda: last.run(lin.data_ptr(), lf_ptr, ly.data_ptr(), stream),
+        "gflop_per_step": gflop, "gflop_per_launch": last_gflop,
+        "h2d": hx.numel() * 4, "d2h": hy.numel() * 4,
+        "metric": "GFLOP/s", "unit": "GFLOP/s", "precision": "fp32" if prec == _lib.PREC_FP32 else "bf16x3",
+        "plan_algo": last.algo,
+        "config": {"workload": "eight-layer 3x3 stack on 224x224x3 (widths 64,64,128,128,256,256,512,512; "
+                               "DownsampleOutput(2) after layers 2,4,6; ReLU between layers), "
+                               f"batch {B}, one CUDA-graph replay per step",
+                   "batch": B, "layers": 8, "gflop_per_step": round(gflop, 2),
+                   "l2": "activations of batch 64 (1.2 GB per step) exceed the 126 MB L2"},
+        "dtype": "f32" if prec == _lib.PREC_FP32 else "bf16x3 split, f32 accumulate",
+        "keep": (stack, last, lin, lf, ly, hx, hy),
+        "kernel": "frame_tc_kernel (layer 8)" if prec != _lib.PREC_FP32 else "frame_f32_kernel (layer 8)",
+        "extra": extra,
+    }
+
+
 # ----------------------------------------------------------------------------- timing
 def time_steps(fn, steps, warmup, pg):
     """W untimed steps, then K steps between CUDA events, bracketed by a
@@ -342,12 +526,64 @@ def cpu_plain_sample(seconds_budget=10.0):
     return gb * reps / el, threads, f"{reps} x 64 planes of 256x256, {el:.1f} s"
 
 
+def cpu_fft_sample(seconds_budget=10.0):
+    """Oracle direct convolution (the reference's loop order, FP32) of a
+    band of output rows of the 2048x2048 (*) 63x63 cyclic case, all host
+    threads.  GFLOP/s in the same direct-equivalent flops as the GPU line."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+    import oracle as O
+    n, k, band = 2048, 63, 64
+    rng = np.random.default_rng(3)
+    # every output point costs R*S multiply-adds whatever the border, so a
+    # (band + 62) x 2048 cyclic field stands in for a band of the full field
+    x = rng.uniform(0, 1, (band + k - 1, n)).astype(np.float32)
+    f = gaussian_filter(k)
+    d = O.make_desc(band + k - 1, n, k, k, border=O.CYCLIC, orient=O.CONV)
+    threads = os.cpu_count() or 1
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.conv(d, x, f, threads=threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > seconds_budget or reps >= 50:
+            break
+    gflop = 2.0 * (band + k - 1) * n * k * k / 1e9
+    return gflop * reps / el, threads, f"{reps} x ({band + k - 1}x{n} (*) {k}x{k} cyclic), {el:.1f} s"
+
+
+def cpu_graph_sample(seconds_budget=10.0):
+    """Oracle FP32 projectFrameBlockReduceSum of layer 8 of the stack (28x28,
+    512 -> 512 planes, 3x3) for one sample, all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+    import oracle as O
+    rng = np.random.default_rng(5)
+    C = K = 512
+    H = W = 28
+    x = rng.uniform(-1, 1, (C, H, W)).astype(np.float32)
+    f = (rng.standard_normal((K * C, 3, 3)) * np.sqrt(2 / (C * 9))).astype(np.float32)
+    d = O.make_desc(H, W, 3, 3, planes=C, f_planes=K * C, batch=1, border=O.ZERO, orient=O.XCORR,
+                    mode=O.PROJECT_REDUCE)
+    threads = os.cpu_count() or 1
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        O.conv(d, x, f, threads=threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > seconds_budget or reps >= 100:
+            break
+    gflop = 2.0 * K * C * H * W * 9 / 1e9
+    return gflop * reps / el, threads, f"{reps} x layer 8 of one sample (28x28, 512->512, 3x3), {el:.1f} s"
+
+
 # ----------------------------------------------------------------------------- main
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    fn = cpu_frame_sample if args.workload == "frame" else cpu_plain_sample
+    fn = {"frame": cpu_frame_sample, "plain": cpu_plain_sample, "fft": cpu_fft_sample,
+          "graph": cpu_graph_sample}[args.workload]
     per = []
     for _ in range(max(args.warmup, 0)):
         fn(seconds_budget=1.0)
@@ -355,10 +591,14 @@ def run_reference(args):
         v, threads, sample = fn(seconds_budget=2.0)
         per.append(v)
     value = statistics.median(per)
-    unit = "GFLOP/s" if args.workload == "frame" else "GB/s"
-    cfg = {"workload": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 K=64 64x64 "
-                       "5x5 BorderZero" if args.workload == "frame" else
-                       "plain convolve 256x256 (*) 5x5 BorderZero"}
+    unit = "GB/s" if args.workload == "plain" else "GFLOP/s"
+    cfg = {"workload": {
+        "frame": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 K=64 64x64 5x5 "
+                 "BorderZero",
+        "plain": "plain convolve 256x256 (*) 5x5 BorderZero",
+        "fft": "convolve 2048x2048 (*) 63x63 normalised Gaussian (sigma 10), BorderCyclic "
+               "(direct-equivalent flops)",
+        "graph": "eight-layer 3x3 stack on 224x224x3, one layer-8 sample (28x28, 512->512)"}[args.workload]}
     line = {"impl": "reference", "metric": unit, "value": round(value, 3), "unit": unit,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -381,7 +621,8 @@ def main():
     from cctconv import _lib
 
     rank, world, local, pg = dist_setup(args.gpus)
-    wl = frame_workload(args.precision) if args.workload == "frame" else plain_workload()
+    wl = {"frame": lambda: frame_workload(args.precision), "plain": plain_workload,
+          "fft": fft_workload, "graph": lambda: graph_workload(args.precision)}[args.workload]()
     peaks, peak_kind = load_peaks()
 
     with ClockSampler(torch.cuda.current_device()) as clocks:
@@ -393,7 +634,13 @@ def main():
     e2e_t = max_over_ranks(pg, e2e_t)
     e2e_steps = max(args.steps // 20, 3)
 
-    if wl["unit"] == "GFLOP/s":
+    if wl.get("fft_hbm_roofline"):
+        # FFT: reported in direct-equivalent GFLOP/s; its roofline is HBM
+        value = world * wl["gflop_per_step"] * args.steps / t_max
+        e2e_val = world * wl["gflop_per_step"] * e2e_steps / e2e_t
+        achieved = wl["bytes_per_launch"] / per_launch / 1e9
+        bound, peak, unit = "hbm", peaks["hbm_gbs"], "GB/s"
+    elif wl["unit"] == "GFLOP/s":
         value = world * wl["gflop_per_step"] * args.steps / t_max
         e2e_val = world * wl["gflop_per_step"] * e2e_steps / e2e_t
         achieved = wl["gflop_per_launch"] / per_launch / 1e3  # TFLOP/s
@@ -415,7 +662,8 @@ def main():
         return 0
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        fn = cpu_frame_sample if wl["unit"] == "GFLOP/s" else cpu_plain_sample
+        fn = {"frame": cpu_frame_sample, "plain": cpu_plain_sample,
+              "fft": cpu_fft_sample, "graph": cpu_graph_sample}[args.workload]
         v, threads, sample = fn(seconds_budget=10.0)
         cpu = {"value": round(v, 3), "unit": wl["unit"], "cores": threads, "kind": "port",
                "sample": sample}
@@ -436,6 +684,7 @@ def main():
         "clocks": clocks.summary(),
         "plan_algo": wl["plan_algo"],
     }
+    line.update(wl.get("extra", {}))
     print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

@@ -71,6 +71,14 @@ SIGNATURES = {
     "cct_conv_run_host": (_I, [_P, _P, _P, _P, _P]),
     "cct_conv_separable": (_I, [_I32, _I32, _I32, _P, _P, _I32, _P, _I32, _I32, _I32, _P, _P, _P]),
     "cct_conv_run_noalloc": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P]),
+    "cct_graph_create": (_I, [ctypes.POINTER(ConvDesc), _I32, ctypes.POINTER(_P)]),
+    "cct_graph_destroy": (_I, [_P]),
+    "cct_graph_set_filter": (_I, [_P, _I32, _P]),
+    "cct_graph_field": (_I, [_P, _I32, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_graph_step": (_I, [_P, ctypes.c_int64, _P]),
+    "cct_graph_step_host": (_I, [_P, _P, _P, _P]),
+    "cct_graph_time": (ctypes.c_int64, [_P]),
+    "cct_graph_reset": (_I, [_P]),
     "cct_malloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
     "cct_free": (_I, [_P]),
     "cct_memcpy_h2d": (_I, [_P, _P, ctypes.c_size_t, _P]),
@@ -147,6 +155,55 @@ class Plan:
     def close(self):
         if self.handle:
             LIB.cct_conv_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """Owning wrapper of a cct_graph: a chain of convolution layers stepped
+    as one captured launch sequence."""
+
+    def __init__(self, descs):
+        arr = (ConvDesc * len(descs))(*descs)
+        h = ctypes.c_void_p()
+        check(LIB.cct_graph_create(arr, len(descs), ctypes.byref(h)))
+        self.handle = h
+        self.descs = list(descs)
+        self.shapes = [output_shape(d) for d in descs]
+
+    def set_filter(self, layer, host_ptr):
+        check(LIB.cct_graph_set_filter(self.handle, layer, ctypes.c_void_p(host_ptr)))
+
+    def field(self, index):
+        """(device pointer, element count) of field `index` (0 = input)."""
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        check(LIB.cct_graph_field(self.handle, index, ctypes.byref(p), ctypes.byref(n)))
+        return p.value, n.value
+
+    def step(self, count=1, stream=0):
+        check(LIB.cct_graph_step(self.handle, count, ctypes.c_void_p(stream)))
+        return self.time
+
+    def step_host(self, in_ptr, out_ptr, stream=0):
+        check(LIB.cct_graph_step_host(self.handle, ctypes.c_void_p(in_ptr), ctypes.c_void_p(out_ptr),
+                                      ctypes.c_void_p(stream)))
+
+    @property
+    def time(self):
+        return int(LIB.cct_graph_time(self.handle))
+
+    def reset(self):
+        check(LIB.cct_graph_reset(self.handle))
+        return 0
+
+    def close(self):
+        if self.handle:
+            LIB.cct_graph_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

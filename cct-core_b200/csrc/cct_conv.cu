@@ -11,8 +11,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "cct_internal.h"
+#include "fft_conv.h"
 #include "frame_tc.h"
 
 namespace cct {
@@ -34,7 +36,13 @@ int check_cuda(cudaError_t e, const char *what) {
   return set_error(status, "%s: %s", what, cudaGetErrorString(e));
 }
 
-void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// Launches issued while this thread captures a CUDA graph are not counted
+// (nothing runs); each replay of the graph counts its kernel nodes instead.
+static thread_local bool t_capturing = false;
+void count_launches(uint64_t n) {
+  if (!t_capturing) g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+void set_launch_capture(bool on) { t_capturing = on; }
 
 static std::mutex g_err_mu;
 static unsigned *g_err_word[64];
@@ -180,6 +188,11 @@ struct cct_conv_plan {
   TcParams tc;           // tensor-core tile plan (ALGO_FRAME_BF16X3)
   uint8_t *packed;       // packed bf16 hi/lo filter operand (plan workspace)
   bool packed_static;    // packed holds the static filter
+  FftParams fft;         // FFT plan (ALGO_FFT)
+  float2 *fft_spec;      // working spectrum (plan workspace)
+  float2 *fft_filter;    // filter spectrum
+  float2 *fft_tw;        // twiddle tables
+  bool fft_static;       // fft_filter holds the static filter's FP64 spectrum
   // run_host staging (allocated on the first cct_conv_run_host call)
   float *d_x, *d_f, *d_y;
 };
@@ -240,14 +253,29 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   int algo;
   const bool reduce = g.mode == CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM ||
                       g.mode == CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM;
-  if (d->algo == CCT_ALGO_FFT)
-    return set_error(CCT_ENOTSUP, "FFT convolution not available in this build");
+  // Direct vs FFT (DynamicConvolutionGenerator.scala:109-150): the FFT takes
+  // plane-by-plane convolutions without sampling under Zero/Clamp/Cyclic;
+  // UseFFTAlways falls back to the direct kernels outside that, as the
+  // reference does; WhenBest compares modelled times.
+  FftParams fp{};
+  bool use_fft = false;
+  if (d->algo != CCT_ALGO_DIRECT && fft_plan(g, &fp)) {
+    if (d->algo == CCT_ALGO_FFT) {
+      use_fft = true;
+    } else {
+      const double direct_s = 2.0 * g.OH * g.OW * g.R * g.S * (double)g.pout / 30e12 + 3e-6;
+      const double fft_s = 24.0 * fp.Fr * fp.Fc * (double)g.pout / 2e12 + 12e-6;
+      use_fft = fft_s < direct_s;
+    }
+  }
   TcParams tc{};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (d->precision == CCT_PREC_BF16X3 && !reduce)
     return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
-  if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
+  if (use_fft)
+    algo = ALGO_FFT;
+  else if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
     algo = ALGO_FRAME_BF16X3;
   else
     algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
@@ -273,6 +301,25 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
       return rc;
     }
   }
+  if (algo == ALGO_FFT) {
+    p->fft = fp;
+    rc = check_cuda(cudaMalloc(&p->fft_spec, fp.spec_elems * sizeof(float2)), "cudaMalloc(fft spectrum)");
+    if (!rc)
+      rc = check_cuda(cudaMalloc(&p->fft_filter, fp.filter_elems * sizeof(float2)),
+                      "cudaMalloc(fft filter spectrum)");
+    if (!rc) rc = check_cuda(cudaMalloc(&p->fft_tw, fp.tw_elems * sizeof(float2)), "cudaMalloc(fft twiddles)");
+    if (!rc) {
+      std::vector<float> tw;
+      fft_twiddles(fp, &tw);
+      rc = check_cuda(cudaMemcpy(p->fft_tw, tw.data(), tw.size() * sizeof(float), cudaMemcpyHostToDevice),
+                      "cudaMemcpy(fft twiddles)");
+    }
+    if (rc) {
+      cct_conv_plan_destroy(p);
+      return rc;
+    }
+    fft_set_tables(&p->fft, p->fft_tw);
+  }
   *out = p;
   return CCT_OK;
 }
@@ -281,6 +328,9 @@ int cct_conv_plan_destroy(cct_conv_plan *p) {
   if (!p) return CCT_OK;
   cudaFree(p->static_filter);
   cudaFree(p->packed);
+  cudaFree(p->fft_spec);
+  cudaFree(p->fft_filter);
+  cudaFree(p->fft_tw);
   cudaFree(p->d_x);
   cudaFree(p->d_f);
   cudaFree(p->d_y);
@@ -304,6 +354,16 @@ int cct_conv_plan_set_static_filter(cct_conv_plan *p, const float *host_filter) 
   int rc = check_cuda(cudaMemcpy(p->static_filter, host_filter, bytes, cudaMemcpyHostToDevice),
                       "cudaMemcpy(static filter)");
   if (rc) return rc;
+  if (p->algo == ALGO_FFT) {
+    // the reference transforms constant filters on the host in FP64
+    // (DynamicConvolutionGenerator.scala:342-350, 376-405)
+    std::vector<float> spec;
+    fft_static_spectrum(p->fft, host_filter, &spec);
+    rc = check_cuda(cudaMemcpy(p->fft_filter, spec.data(), spec.size() * sizeof(float), cudaMemcpyHostToDevice),
+                    "cudaMemcpy(static filter spectrum)");
+    if (rc) return rc;
+    p->fft_static = true;
+  }
   if (p->algo == ALGO_FRAME_BF16X3) {
     rc = launch_pack_filters(p->tc, p->static_filter, p->packed, 0);
     if (!rc) rc = check_cuda(cudaStreamSynchronize(0), "pack static filter");
@@ -329,6 +389,13 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
     }
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);
+    case ALGO_FFT: {
+      int rc = CCT_OK;
+      if (f != p->static_filter || !p->fft_static)
+        rc = launch_fft_filter_spectrum(p->fft, f, p->fft_filter, st);
+      if (rc) return rc;
+      return launch_fft_conv(p->fft, x, p->fft_filter, p->fft_spec, y, st);
+    }
     default:
       if (direct_tma_supported(p->g, x)) return launch_direct_tma(p->g, x, f, y, st, p->err);
       return launch_direct(p->g, x, f, y, st);

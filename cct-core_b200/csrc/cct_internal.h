@@ -75,6 +75,7 @@ int resolve_geom(const cct_conv_desc *desc, ConvGeom *g);
 int set_error(int status, const char *fmt, ...);
 int check_cuda(cudaError_t e, const char *what);
 void count_launches(uint64_t n);
+void set_launch_capture(bool on);
 
 // Kernel families (each returns CCT_OK or an error status).
 int launch_direct(const ConvGeom &g, const float *x, const float *f, float *y,

@@ -167,6 +167,39 @@ int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes,
 int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *image,
                          const float *filter, float *out, void *stream);
 
+/* ---- stacked convolution graphs (ComputeGraph step) --------------------- */
+/* A ComputeGraph whose fields form a chain of convolutions: layer i reads
+ * layer i-1's output field.  Replaces the reference's ComputeGraph
+ * construction and its evaluator's per-kernel dispatch for such graphs
+ * (src/main/scala/cogx/runtime/ComputeGraph.scala:56, step :228-279,
+ * reset :288): the layers' launches are captured once into a CUDA graph and
+ * every step replays it.  The graph owns every field: the input field
+ * (index 0) and each layer's output (index i); filters are static (the
+ * reference's constant filter fields), set once per layer.
+ *
+ * cct_graph_create   layer descriptors; each layer's image shape must equal
+ *                    the previous layer's output shape.  CCT_EINVAL with a
+ *                    message naming the layer otherwise.
+ * cct_graph_set_filter  host filter of one layer (as cct_conv_plan_set_static_filter).
+ * cct_graph_field    device pointer and element count of field `index`.
+ * cct_graph_step     `count` steps on `stream` (asynchronous; the first step
+ *                    captures the launch sequence, and fails with CCT_EINVAL
+ *                    while a layer has no filter).  Kernel-side timeouts are
+ *                    reported by cct_device_status.
+ * cct_graph_step_host  one step from a host input to the host copy of the
+ *                    last layer's output (synchronous).
+ * cct_graph_time     steps taken since creation or the last reset.
+ * cct_graph_reset    sets the step count to 0 (the fields keep their values). */
+typedef struct cct_graph cct_graph;
+int cct_graph_create(const cct_conv_desc *layers, int32_t n_layers, cct_graph **out);
+int cct_graph_destroy(cct_graph *graph);
+int cct_graph_set_filter(cct_graph *graph, int32_t layer, const float *host_filter);
+int cct_graph_field(const cct_graph *graph, int32_t index, float **device_ptr, size_t *elems);
+int cct_graph_step(cct_graph *graph, int64_t count, void *stream);
+int cct_graph_step_host(cct_graph *graph, const float *host_in, float *host_out, void *stream);
+int64_t cct_graph_time(const cct_graph *graph);
+int cct_graph_reset(cct_graph *graph);
+
 /* ---- device memory helpers (the JNI side has no CUDA runtime) ----------- */
 int cct_malloc(void **ptr, size_t bytes);
 int cct_free(void *ptr);

@@ -17,12 +17,14 @@
 //              (tcgen05.st, row m = lane m): four chunks are in flight.
 //   warp 16    MMA issuer (one elected lane): per 16-deep k-step of a chunk,
 //              with A from tensor memory and B from shared memory,
-//                NT <= 64: A_hi x [B_hi; B_lo] (N = 2*NT) then A_lo x B_hi
-//                          (N = NT) into the first half: the epilogue adds
-//                          the two halves (a tcgen05.mma costs ~46 cycles
-//                          however narrow, so wide N pays);
-//                NT > 64:  A_hi x B_hi, A_hi x B_lo, A_lo x B_hi (N = NT);
-//              into a double-buffered FP32 accumulator in tensor memory.
+//                A_hi x [B_hi; B_lo] (N = 2*NT) into [hh | small], then
+//                A_lo x B_hi (N = NT) into the second half, so the two
+//                small products never meet the large hi*hi sum (the tensor
+//                core's FP32 accumulation would round them against it);
+//                the epilogue adds the halves.  A tcgen05.mma costs ~46
+//                cycles however narrow, so the wide first MMA pays.  The
+//                double-buffered [hh | small] accumulator is 4*NT columns,
+//                so NT <= 64.
 //   warp 17    loader: 3-D TMA loads of the halo tile (zero fill at the
 //              border) and bulk copies of the pre-packed filter chunks.
 //   warps 18-21 epilogue: tcgen05.ld of the accumulator, optional ReLU,
@@ -111,8 +113,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int RS = g.R * g.S;
   const int npix = g.OH * g.OW;
-  const bool concat = p.NT <= 64;                 // [B_hi; B_lo] in one MMA
-  const uint32_t dw = concat ? 2u * p.NT : (uint32_t)p.NT;  // accumulator width
+  const uint32_t dw = 2u * p.NT;  // accumulator width: [hh | small]
   auto d_col = [&](int d) { return d ? dw : 0u; };
   const uint32_t a_col0 = 2u * dw;  // stage s: hi at a_col0 + s*CB, lo at + CB/2
   volatile int *abort_flag = &bars.abort_flag;
@@ -215,7 +216,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t idesc_n = idesc_bf16_f32(kMT, p.NT);
     const uint32_t idesc_2n = idesc_bf16_f32(kMT, 2 * p.NT);
     const uint32_t lbo = 128, sbo = CB * 16;
-    const uint32_t img_bytes = (uint32_t)p.NT * CB * 2;
     const uint32_t bstage0 = smem_u32(bstage);
     uint32_t q = 0, tc = 0;
     bool failed = false;
@@ -235,21 +235,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t a_hi = tmem + a_col0 + (uint32_t)s * CB;
         const uint32_t a_lo = a_hi + CB / 2;
         const uint32_t b_hi = bstage0 + (uint32_t)s * bstage_bytes;
-        const uint32_t b_lo = b_hi + img_bytes;
         if (elect_one()) {
 #pragma unroll
           for (int j = 0; j < CB / 16; ++j) {
             const uint32_t acc = (k > 0 || j > 0) ? 1u : 0u;
             const uint64_t dh = smem_desc_kmajor(b_hi + 256u * j, lbo, sbo);
-            if (concat) {
-              mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_2n, acc);  // [hi*hi | hi*lo]
-              mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc_n, 1u);    // + lo*hi
-            } else {
-              const uint64_t dl = smem_desc_kmajor(b_lo + 256u * j, lbo, sbo);
-              mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_n, acc);
-              mma_bf16_ts(dt, a_hi + 8u * j, dl, idesc_n, 1u);
-              mma_bf16_ts(dt, a_lo + 8u * j, dh, idesc_n, 1u);
-            }
+            mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_2n, acc);       // [hi*hi | hi*lo]
+            mma_bf16_ts(dt + p.NT, a_lo + 8u * j, dh, idesc_n, 1u);  // small half += lo*hi
           }
           tc_commit(&bars.empty[s]);
         }
@@ -347,14 +339,14 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int c = 0; c < p.NT; c += 16) {
         uint32_t v[16], v2[16];
         tmem_ld16(tmem + lane_base + d_col(d) + c, v);
-        if (concat) tmem_ld16(tmem + lane_base + d_col(d) + p.NT + c, v2);
+        tmem_ld16(tmem + lane_base + d_col(d) + p.NT + c, v2);
         tc_wait_ld();
         if (valid) {
 #pragma unroll
           for (int t = 0; t < 16; ++t) {
             if (n0 + c + t < g.groups) {
               float val = __uint_as_float(v[t]);
-              if (concat) val += __uint_as_float(v2[t]);
+              val += __uint_as_float(v2[t]);
               if (relu) val = fmaxf(val, 0.0f);
               ybase[(size_t)(c + t) * npix] = val;
             }
@@ -459,7 +451,7 @@ bool frame_tc_plan(const ConvGeom &g, int sms, TcParams *out) {
   p.g = g;
   const int npix = g.OH * g.OW;
   p.tiles_m = (npix + kMT - 1) / kMT;
-  p.NT = std::min(128, ((g.groups + 15) / 16) * 16);
+  p.NT = std::min(64, ((g.groups + 15) / 16) * 16);
   p.nblocks = (g.groups + p.NT - 1) / p.NT;
   p.total_tiles = g.batch * p.tiles_m * p.nblocks;
   // rows of output spanned by any tile
@@ -482,7 +474,7 @@ bool frame_tc_plan(const ConvGeom &g, int sms, TcParams *out) {
     if (cb > cmax && cb != 16) continue;
     const size_t halo = (((size_t)p.TC * p.TR * cb * 4) + 1023) & ~(size_t)1023;
     const size_t bst = (size_t)kStages * 2u * p.NT * cb * 2;
-    const int dw = p.NT <= 64 ? 2 * p.NT : p.NT;
+    const int dw = 2 * p.NT;
     const int tcols = 2 * dw + kStages * cb;
     if (2 * halo + bst <= budget && tcols <= 512) {
       p.CB = cb;

@@ -14,7 +14,9 @@ normalised Gaussian, sigma 10, BorderCyclic, through the FFT path, with its
 max/RMS error against an FP64 FFT and the direct kernel's time beside it);
 graph (the eight-layer 3x3 stack on 224x224x3, widths 64..512, stepped as
 one captured launch sequence; batch 64 headline, batches 1 and 8 and FP32
-beside it).
+beside it); serve (10,000 seeded convolve/projectFrame requests of uneven
+sizes with Poisson arrivals, served with continuous batching and with plain
+per-call dispatch: throughput and p50/p99 latency, rate swept 1k-50k/s).
 
 Prints one JSON line (rank 0).  Multi-GPU: replicas only -- every rank runs
 the same step on its own GPU; value = all ranks' work / max rank time.
@@ -40,9 +42,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["frame", "plain", "fft", "graph"], default="frame")
+    ap.add_argument("--workload", choices=["frame", "plain", "fft", "graph", "serve"], default="frame")
     ap.add_argument("--precision", choices=["auto", "fp32", "bf16x3"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
     return ap.parse_args()
 
 
@@ -420,6 +424,110 @@ def graph_workload(precision):
     }
 
 
+def serve_requests(n, seed=5):
+    """n seeded request specs: side log-uniform in [32, 1024], filter size
+    from {3,5,7,9}, planes from {1,4,16,64}, filters from {1,16,64}."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    side = np.exp(rng.uniform(np.log(32), np.log(1024), n)).astype(int)
+    R = rng.choice([3, 5, 7, 9], n)
+    C = rng.choice([1, 4, 16, 64], n)
+    K = rng.choice([1, 16, 64], n)
+    return [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(side, R, C, K)]
+
+
+def run_serve(args):
+    """Continuous batching vs plain per-call dispatch on the same request
+    stream (rank 0 only; every rank serves its own stream under torchrun)."""
+    import numpy as np
+    import torch
+    from cctconv import _lib
+    from cctconv.serve import Server, conv_request
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    rng = np.random.default_rng(5)
+    specs = serve_requests(args.serve_requests)
+    max_in = max(s * s * c for s, r, c, k in specs)
+    max_out = max(s * s * (c if k == 1 else k) for s, r, c, k in specs)
+    # one shared input pool (requests read its start) and a ring of output space
+    pool = torch.from_numpy(rng.uniform(-1, 1, max_in).astype(np.float32)).pin_memory()
+    ring_elems = max(4 * max_out, 1 << 29)
+    ring = torch.empty(ring_elems).pin_memory()
+
+    def build(server):
+        banks, reqs, flops, hbytes = {}, [], 0.0, 0
+        pos = 0
+        for side, R, C, K in specs:
+            key = (R, C, K)
+            if key not in banks:
+                fp = 1 if K == 1 else K * C
+                banks[key] = server.add_filter(rng.uniform(-1, 1, (fp, R, R)).astype(np.float32))
+            if K == 1:
+                d = _lib.new_desc(image_rows=side, image_cols=side, image_planes=C if C > 1 else 0,
+                                  filter_rows=R, filter_cols=R, filter_planes=0,
+                                  orientation=_lib.CONVOLUTION, vector_mode=_lib.PLANE_BY_PLANE)
+                planes = C
+            else:
+                d = _lib.new_desc(image_rows=side, image_cols=side, image_planes=C, filter_rows=R,
+                                  filter_cols=R, filter_planes=K * C, orientation=_lib.CROSS_CORRELATION,
+                                  vector_mode=_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM)
+                planes = K
+            out = side * side * planes
+            if pos + out > ring_elems:
+                pos = 0
+            reqs.append(conv_request(d, pool.data_ptr(), ring.data_ptr() + 4 * pos, None, banks[key]))
+            pos += (out + 63) // 64 * 64
+            flops += 2.0 * side * side * planes * R * R * (C if K > 1 else 1)
+            hbytes += 4 * side * side * (C + planes)
+        return reqs, flops, hbytes
+
+    def run(per_call, rate, n):
+        server = Server(slots=4, max_batch=64, arena_bytes=16 << 30, per_call=per_call)
+        reqs, flops, hbytes = build(server)
+        reqs, k = reqs[:n], n / len(reqs)
+        arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))
+        t0 = time.perf_counter()
+        lat = server.replay(reqs, arrivals)
+        wall = time.perf_counter() - t0
+        st = server.stats()
+        server.close()
+        return {"rate": rate, "requests": n, "served_per_s": round(n / wall, 1),
+                "p50_ms": round(float(np.percentile(lat, 50)) / 1e3, 3),
+                "p99_ms": round(float(np.percentile(lat, 99)) / 1e3, 3),
+                "GFLOP/s": round(flops * k / wall / 1e9, 1), "host_GB/s": round(hbytes * k / wall / 1e9, 2),
+                "batches": st["batches"], "solo": st["solo"]}
+
+    head = run(False, args.serve_rate, args.serve_requests)
+    base = run(True, args.serve_rate, min(args.serve_requests, 3000))
+    sweep = []
+    for rate in (1000.0, 2000.0, 5000.0, 10000.0, 20000.0, 50000.0):
+        n = min(args.serve_requests, 1500)
+        sweep.append({"batched": run(False, rate, n), "per_call": run(True, rate, n)})
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+    line = {
+        "metric": "served requests/s", "value": round(head["served_per_s"] * world, 1), "unit": "req/s",
+        "n_gpus": world, "steps": args.serve_requests, "warmup": 0,
+        "ms_per_step": round(1e3 / head["served_per_s"], 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.serve_requests} requests, Poisson arrivals at {args.serve_rate:g}/s, "
+                               "side log-uniform 32-1024, R {3,5,7,9}, planes {1,4,16,64}, "
+                               "filters {1,16,64}, FP32 host I/O, resident filter banks",
+                   "parallelism": f"replicas{world}"},
+        "latency": {"p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"]},
+        "per_call": base, "batched": head, "sweep": sweep,
+        "e2e": {"value": round(head["served_per_s"] * world, 1), "unit": "req/s",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
+        "gpu_launches": int(head["batches"] + head["solo"]),
+    }
+    print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 # ----------------------------------------------------------------------------- timing
 def time_steps(fn, steps, warmup, pg):
     """W untimed steps, then K steps between CUDA events, bracketed by a
@@ -582,6 +690,10 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    if args.workload == "serve":
+        print(json.dumps({"impl": "reference", "unavailable": "cct-core has no request-serving path; "
+                          "the serve line reports plain per-call dispatch beside batching"}), flush=True)
+        return 0
     fn = {"frame": cpu_frame_sample, "plain": cpu_plain_sample, "fft": cpu_fft_sample,
           "graph": cpu_graph_sample}[args.workload]
     per = []
@@ -617,6 +729,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serve":
+        return run_serve(args)
     import torch
     from cctconv import _lib
 

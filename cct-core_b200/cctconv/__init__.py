@@ -32,7 +32,8 @@ __all__ = [
     "UseFFTNever", "UseFFTAlways", "UseFFTWhenBest",
     "convolve", "crossCorrelate", "convolveSeparable", "crossCorrelateSeparable",
     "projectFrame", "projectFrameBlockReduceSum", "backProjectFrame",
-    "backProjectFrameBlockReduceSum", "make_desc", "plan_for", "CctError", "Plan",
+    "backProjectFrameBlockReduceSum", "crossCorrelateFilterAdjoint", "convolveFilterAdjoint",
+    "filterAdjointBlockReduceSum", "make_desc", "plan_for", "CctError", "Plan",
 ]
 
 
@@ -146,8 +147,11 @@ def _run(field, filt, border, orientation, sampling, mode, batch, precision=_lib
     # ScalarField result when both inputs are scalar (plane-by-plane), and the
     # length-1 BlockReduceSum result is sliced to a ScalarField
     # (CogFunctionAPI.scala:1406-1409, 1461-1464).
+    # ...and a FilterAdjoint result of one plane is a ScalarField
+    # (ConvolveHyperKernel.scala:1414-1429).
     squeeze = (fs[2] == 0 and ks[2] == 0) or (
-        mode in (_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, _lib.BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+        mode in (_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, _lib.BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM,
+                 _lib.FILTER_ADJOINT, _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM)
         and planes == 1)
     y = _out_tensor(shape, planes, field, squeeze, field.dim() == 1)
     stream = torch.cuda.current_stream(field.device).cuda_stream
@@ -188,6 +192,33 @@ def backProjectFrameBlockReduceSum(field, filter, borderPolicy,
                                    precision=_lib.PREC_FP32, relu=False):
     return _run(field, filter, borderPolicy, _lib.CONVOLUTION, samplingPolicy,
                 _lib.BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM, batchSize, precision, relu=relu)
+
+
+def crossCorrelateFilterAdjoint(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
+                                batchSize=1):
+    """Weight-gradient plane mixing (CogFunctionAPI.scala:1480-1487): `filter`
+    is the gradient field of batchSize*L planes; output plane B*w + b,
+    w = l*C + c, correlates image plane b*C + c with gradient plane b*L + l.
+    UpsampleInput upsamples the gradient."""
+    return _run(field, filter, borderPolicy, _lib.CROSS_CORRELATION, samplingPolicy,
+                _lib.FILTER_ADJOINT, batchSize)
+
+
+def convolveFilterAdjoint(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
+                          batchSize=1):
+    """As crossCorrelateFilterAdjoint with the (upsampled) gradient flipped
+    (CogFunctionAPI.scala:1503-1510)."""
+    return _run(field, filter, borderPolicy, _lib.CONVOLUTION, samplingPolicy,
+                _lib.FILTER_ADJOINT, batchSize)
+
+
+def filterAdjointBlockReduceSum(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
+                                batchSize=1, orientation=_lib.CROSS_CORRELATION):
+    """blockReduceSum(crossCorrelateFilterAdjoint(...), batchSize) fused, the
+    form the reference's optimizer emits (FilterAdjointBlockReduceSum): plane
+    w sums the batchSize images' planes in order."""
+    return _run(field, filter, borderPolicy, orientation, samplingPolicy,
+                _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM, batchSize)
 
 
 def _separable(field, rowFilter, columnFilter, borderPolicy, orientation):

@@ -18,7 +18,7 @@ BORDER_ZERO, BORDER_CLAMP, BORDER_CYCLIC, BORDER_VALID, BORDER_FULL = range(5)
 CROSS_CORRELATION, CONVOLUTION = 0, 1
 SAMPLE_NONE, SAMPLE_DOWN, SAMPLE_UP = 0, 1, 2
 (PLANE_BY_PLANE, PROJECT_FRAME, PROJECT_FRAME_BLOCK_REDUCE_SUM, BACK_PROJECT_FRAME,
- BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM) = range(5)
+ BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM, FILTER_ADJOINT, FILTER_ADJOINT_BLOCK_REDUCE_SUM) = range(7)
 PREC_FP32, PREC_BF16X3 = 0, 1
 ALGO_AUTO, ALGO_DIRECT, ALGO_FFT = 0, 1, 2
 FLAG_RELU = 0x1
@@ -55,6 +55,22 @@ class CctError(RuntimeError):
         self.status = status
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_int32), ("slots", ctypes.c_int32),
+                ("max_batch", ctypes.c_int32), ("flags", ctypes.c_int32),
+                ("arena_bytes", ctypes.c_uint64)]
+
+
+class ServeRequest(ctypes.Structure):
+    _fields_ = [("struct_size", ctypes.c_int32), ("kind", ctypes.c_int32), ("desc", ConvDesc),
+                ("image", ctypes.c_void_p), ("filter", ctypes.c_void_p),
+                ("filter_id", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("out", ctypes.c_void_p), ("graph", ctypes.c_void_p)]
+
+
+SERVE_CONV, SERVE_GRAPH_STEP = 0, 1
+SERVE_PER_CALL = 0x1
+
 # Every symbol include/cct_conv.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -79,6 +95,18 @@ SIGNATURES = {
     "cct_graph_step_host": (_I, [_P, _P, _P, _P]),
     "cct_graph_time": (ctypes.c_int64, [_P]),
     "cct_graph_reset": (_I, [_P]),
+    "cct_server_config_init": (None, [ctypes.POINTER(ServerConfig)]),
+    "cct_serve_request_init": (None, [ctypes.POINTER(ServeRequest)]),
+    "cct_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
+    "cct_server_destroy": (_I, [_P]),
+    "cct_server_add_filter": (_I, [_P, _P, ctypes.c_size_t, _PI32]),
+    "cct_server_submit": (_I, [_P, ctypes.POINTER(ServeRequest), ctypes.POINTER(ctypes.c_uint64)]),
+    "cct_server_wait": (_I, [_P, ctypes.c_uint64, _I32, ctypes.POINTER(ctypes.c_double)]),
+    "cct_server_replay": (_I, [_P, ctypes.POINTER(ServeRequest), ctypes.POINTER(ctypes.c_double), _I32,
+                               ctypes.POINTER(ctypes.c_double)]),
+    "cct_server_stats": (_I, [_P] + [ctypes.POINTER(ctypes.c_uint64)] * 4),
+    "cct_host_alloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
+    "cct_host_free": (_I, [_P]),
     "cct_malloc": (_I, [ctypes.POINTER(_P), ctypes.c_size_t]),
     "cct_free": (_I, [_P]),
     "cct_memcpy_h2d": (_I, [_P, _P, ctypes.c_size_t, _P]),

@@ -78,7 +78,7 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
     return set_error(CCT_EINVAL, "bad border policy %d", d->border);
   if (d->orientation != CCT_CROSS_CORRELATION && d->orientation != CCT_CONVOLUTION)
     return set_error(CCT_EINVAL, "bad filter orientation %d", d->orientation);
-  if (d->vector_mode < CCT_PLANE_BY_PLANE || d->vector_mode > CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+  if (d->vector_mode < CCT_PLANE_BY_PLANE || d->vector_mode > CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM)
     return set_error(CCT_EINVAL, "bad vector mode %d", d->vector_mode);
   if (d->precision != CCT_PREC_FP32 && d->precision != CCT_PREC_BF16X3)
     return set_error(CCT_EINVAL, "bad precision %d", d->precision);
@@ -110,11 +110,16 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
   if (sampling == CCT_SAMPLE_UP && d->border == CCT_BORDER_CLAMP)
     return set_error(CCT_EINVAL, "Integrated upsampling with BorderClamp convolution not supported");
 
+  // FilterAdjoint upsamples its second operand (the gradient), not the
+  // image (ConvolveHyperKernel.scala:1306-1326).
+  const bool fa = d->vector_mode == CCT_FILTER_ADJOINT || d->vector_mode == CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM;
+  const int fup = (fa && sampling == CCT_SAMPLE_UP) ? step : 1;
+  const int Re = R * fup, Se = S * fup;
   long long ur = d->image_rows, uc = d->image_cols;
-  if (sampling == CCT_SAMPLE_UP) { ur *= step; uc *= step; }
+  if (sampling == CCT_SAMPLE_UP && !fa) { ur *= step; uc *= step; }
   long long orow = ur, ocol = uc;
-  if (d->border == CCT_BORDER_VALID) { orow = ur - R + 1; ocol = uc - S + 1; }
-  if (d->border == CCT_BORDER_FULL) { orow = ur + R - 1; ocol = uc + S - 1; }
+  if (d->border == CCT_BORDER_VALID) { orow = ur - Re + 1; ocol = uc - Se + 1; }
+  if (d->border == CCT_BORDER_FULL) { orow = ur + Re - 1; ocol = uc + Se - 1; }
   if (orow < 1 || ocol < 1) return set_error(CCT_EINVAL, "BorderValid filter larger than the input");
   if (sampling == CCT_SAMPLE_DOWN) { orow = (orow + step - 1) / step; ocol = (ocol + step - 1) / step; }
   if (orow > (1 << 30) || ocol > (1 << 30)) return set_error(CCT_EINVAL, "output too large");
@@ -128,6 +133,22 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
       return set_error(CCT_EINVAL,
                        "plane-by-plane convolution needs a ScalarField operand or equal tensor shapes");
     pout = d->image_planes == 0 ? pf : pin;
+  } else if (fa) {
+    // ConvolveHyperKernel.scala:1366-1377 (checks) and 1414-1429 (output planes)
+    if (pf % batch != 0)
+      return set_error(CCT_EINVAL, "Filter tensorshape points %d must be a multiple of the batchSize %d", pf,
+                       batch);
+    if (pin % batch != 0)
+      return set_error(CCT_EINVAL, "Input tensorshape points %d must be a multiple of the batchSize %d",
+                       pin, batch);
+    n = pin / batch;
+    groups = pf / batch;
+    if (d->vector_mode == CCT_FILTER_ADJOINT) {
+      pout = n * groups * batch;
+    } else {
+      pout = n * groups;
+      terms = batch;
+    }
   } else {
     if (pin % batch != 0)
       return set_error(CCT_EINVAL, "Input tensorshape points %d must be a multiple of the batchSize %d",
@@ -149,14 +170,17 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
   g->W = d->image_cols;
   g->OH = (int)orow;
   g->OW = (int)ocol;
-  g->R = R;
-  g->S = S;
-  g->low_r = d->border == CCT_BORDER_FULL ? R - 1 : (d->border == CCT_BORDER_VALID ? 0 : (R - 1) / 2);
-  g->low_c = d->border == CCT_BORDER_FULL ? S - 1 : (d->border == CCT_BORDER_VALID ? 0 : (S - 1) / 2);
+  g->R = Re;
+  g->S = Se;
+  g->fr = R;
+  g->fs = S;
+  g->fup = fup;
+  g->low_r = d->border == CCT_BORDER_FULL ? Re - 1 : (d->border == CCT_BORDER_VALID ? 0 : (Re - 1) / 2);
+  g->low_c = d->border == CCT_BORDER_FULL ? Se - 1 : (d->border == CCT_BORDER_VALID ? 0 : (Se - 1) / 2);
   g->border = d->border;
   g->orient = d->orientation;
   g->down = sampling == CCT_SAMPLE_DOWN ? step : 1;
-  g->up = sampling == CCT_SAMPLE_UP ? step : 1;
+  g->up = (sampling == CCT_SAMPLE_UP && !fa) ? step : 1;
   g->mode = d->vector_mode;
   g->pin = pin;
   g->pf = pf;
@@ -291,7 +315,7 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   p->device = dev;
   p->err = err_word;
   p->x_elems = (size_t)g.pin * g.H * g.W;
-  p->f_elems = (size_t)g.pf * g.R * g.S;
+  p->f_elems = (size_t)g.pf * g.fr * g.fs;
   p->y_elems = (size_t)g.pout * g.OH * g.OW;
   p->tc = tc;
   if (algo == ALGO_FRAME_BF16X3) {

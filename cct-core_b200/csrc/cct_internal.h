@@ -16,7 +16,7 @@ namespace cct {
 struct ConvGeom {
   int H, W;          // input plane (pre-sampling)
   int OH, OW;        // output plane
-  int R, S;          // filter plane
+  int R, S;          // filter plane (FilterAdjoint + UpsampleInput: the upsampled size)
   int low_r, low_c;  // low halo (ConvolveHyperKernel.scala:824-830)
   int border;        // CCT_BORDER_*
   int orient;        // CCT_CROSS_CORRELATION / CCT_CONVOLUTION
@@ -29,6 +29,8 @@ struct ConvGeom {
   int groups;        // filters per image: pf / n (frame modes)
   int terms;         // planes summed per output plane (n for *_REDUCE, else 1)
   uint32_t flags;
+  int fr, fs;        // filter plane as stored (R = fr * fup, S = fs * fup)
+  int fup;           // FilterAdjoint + UpsampleInput: the gradient's upsampling step, else 1
 };
 
 // Plane mixing of ConvolveHyperKernel (ConvolveHyperKernel.scala:124-199,
@@ -58,10 +60,21 @@ __host__ __device__ inline void plane_pair(const ConvGeom &g, int o, int t,
       *fp = g.groups * (w % g.n) + w / g.n;
       break;
     }
-    default: {  // CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM
+    case CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM: {
       int b = o / g.groups, l = o - b * g.groups;
       *ip = b * g.n + t;
       *fp = t * g.groups + l;
+      break;
+    }
+    case CCT_FILTER_ADJOINT: {  // out B*w + b, w = l*C + c (ConvolveHyperKernel.scala:187, 333, 575-590)
+      int b = o % g.batch, w = o / g.batch;
+      *ip = b * g.n + w % g.n;
+      *fp = b * g.groups + w / g.n;
+      break;
+    }
+    default: {  // CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM: out w, term t = image t of the batch
+      *ip = t * g.n + o % g.n;
+      *fp = t * g.groups + o / g.n;
       break;
     }
   }

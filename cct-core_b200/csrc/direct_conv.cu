@@ -153,11 +153,18 @@ __global__ void __launch_bounds__(kThreads)
     int ip, fp;
     plane_pair(g, o, t, &ip, &fp);
     const float *xs = x + (size_t)ip * g.H * g.W;
-    const float *fs = f + (size_t)fp * R * S;
+    const float *fs = f + (size_t)fp * g.fr * g.fs;
     if (t > 0) __syncthreads();
+    // Tap (r, s) of the R x S filter as applied: flipped for convolution, and
+    // for an upsampled FilterAdjoint gradient the zero-inserted lattice
+    // (stored taps at multiples of fup).
     for (int i = threadIdx.x; i < R * S; i += blockDim.x) {
       const int r = i / S, s = i - r * S;
-      wf[i] = __ldg(fs + (g.orient == CCT_CONVOLUTION ? (R - 1 - r) * S + (S - 1 - s) : i));
+      const int er = g.orient == CCT_CONVOLUTION ? R - 1 - r : r;
+      const int es = g.orient == CCT_CONVOLUTION ? S - 1 - s : s;
+      float v = 0.0f;
+      if (er % g.fup == 0 && es % g.fup == 0) v = __ldg(fs + (er / g.fup) * g.fs + es / g.fup);
+      wf[i] = v;
     }
     load_tile(tile, pitch, in_rows, in_cols, xs, g, org_r, org_c);
     __syncthreads();
@@ -240,6 +247,7 @@ int launch_generic(const ConvGeom &g, const float *x, const float *f, float *y,
 
 int launch_direct(const ConvGeom &g, const float *x, const float *f, float *y,
                   cudaStream_t st) {
+  if (g.fup != 1) return launch_generic(g, x, f, y, st);
   if (g.R == g.S && g.down == 1) {
     switch (g.R) {
       case 1: return launch_fixed<1, 1, 1, 4, 4>(g, x, f, y, st);

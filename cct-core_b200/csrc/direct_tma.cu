@@ -254,7 +254,7 @@ int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols,
 }
 
 bool direct_tma_supported(const ConvGeom &g, const float *x) {
-  if (g.terms != 1 || g.up != 1 || g.down != 1) return false;
+  if (g.terms != 1 || g.up != 1 || g.down != 1 || g.fup != 1) return false;
   if (g.border != CCT_BORDER_ZERO && g.border != CCT_BORDER_FULL && g.border != CCT_BORDER_VALID)
     return false;
   if (g.R != g.S || (g.R != 1 && g.R != 3 && g.R != 5 && g.R != 7)) return false;

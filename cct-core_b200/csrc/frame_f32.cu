@@ -190,15 +190,15 @@ bool frame_f32_supported(const ConvGeom &g) {
     return false;
   if (g.R != g.S) return false;
   if (g.down != 1 && g.down != 2) return false;
-  return g.R == 1 || g.R == 3 || g.R == 5 || g.R == 7;
+  return g.R == 1 || g.R == 3 || g.R == 5 || g.R == 7 || g.R == 9;
 }
 
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f, float *y,
                      cudaStream_t st) {
 #define CCT_FRAME_CASE(RR, DD) \
   if (g.R == RR && g.down == DD) return launch<RR, RR, DD>(g, x, f, y, st);
-  CCT_FRAME_CASE(1, 1) CCT_FRAME_CASE(3, 1) CCT_FRAME_CASE(5, 1) CCT_FRAME_CASE(7, 1)
-  CCT_FRAME_CASE(1, 2) CCT_FRAME_CASE(3, 2) CCT_FRAME_CASE(5, 2) CCT_FRAME_CASE(7, 2)
+  CCT_FRAME_CASE(1, 1) CCT_FRAME_CASE(3, 1) CCT_FRAME_CASE(5, 1) CCT_FRAME_CASE(7, 1) CCT_FRAME_CASE(9, 1)
+  CCT_FRAME_CASE(1, 2) CCT_FRAME_CASE(3, 2) CCT_FRAME_CASE(5, 2) CCT_FRAME_CASE(7, 2) CCT_FRAME_CASE(9, 2)
 #undef CCT_FRAME_CASE
   return set_error(CCT_ENOTSUP, "frame FP32 kernel: unsupported filter %dx%d step %d", g.R, g.S,
                    g.down);

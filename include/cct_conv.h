@@ -51,10 +51,18 @@ enum { CCT_BORDER_ZERO = 0, CCT_BORDER_CLAMP = 1, CCT_BORDER_CYCLIC = 2,
 enum { CCT_CROSS_CORRELATION = 0, CCT_CONVOLUTION = 1 };
 /* ConvolutionSamplingPolicy (src/main/scala/cogx/platform/types/ConvolutionSamplingPolicy.scala:27-31) */
 enum { CCT_SAMPLE_NONE = 0, CCT_SAMPLE_DOWN = 1, CCT_SAMPLE_UP = 2 };
-/* VectorMode (src/main/scala/cogx/compiler/parser/op/BinaryOpcode.scala:36-46) */
+/* VectorMode (src/main/scala/cogx/compiler/parser/op/BinaryOpcode.scala:36-46).
+ * FILTER_ADJOINT (crossCorrelateFilterAdjoint / convolveFilterAdjoint,
+ * CogFunctionAPI.scala:1480-1511): the "filter" operand is the gradient field
+ * of batch*L planes; output plane B*w + b (w = l*C + c) is image plane
+ * b*C + c correlated with gradient plane b*L + l (ConvolveHyperKernel.scala
+ * :187, 333, 575-590), and UpsampleInput upsamples the gradient, not the
+ * image (:1313-1326).  FILTER_ADJOINT_BLOCK_REDUCE_SUM sums the B images of
+ * each w in order (the fused blockReduceSum(filterAdjoint(..), B)). */
 enum { CCT_PLANE_BY_PLANE = 0, CCT_PROJECT_FRAME = 1,
        CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM = 2, CCT_BACK_PROJECT_FRAME = 3,
-       CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM = 4 };
+       CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM = 4, CCT_FILTER_ADJOINT = 5,
+       CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM = 6 };
 /* Arithmetic of the multi-plane (frame) kernels.  FP32 is the reference's
  * arithmetic; BF16X3 splits each FP32 operand into bf16 hi+lo and sums the
  * hi*hi + hi*lo + lo*hi products on tcgen05 tensor cores in FP32. */
@@ -199,6 +207,75 @@ int cct_graph_step(cct_graph *graph, int64_t count, void *stream);
 int cct_graph_step_host(cct_graph *graph, const float *host_in, float *host_out, void *stream);
 int64_t cct_graph_time(const cct_graph *graph);
 int cct_graph_reset(cct_graph *graph);
+
+/* ---- request serving (continuous batching) ------------------------------ */
+/* No counterpart in the reference, whose ComputeGraphs are stepped by one
+ * caller at a time.  A server owns one GPU's share of HBM (an arena of
+ * `arena_bytes`) and a scheduler thread.  Requests (a convolution, or a step
+ * of a resident cct_graph) arrive from any thread; each is admitted when
+ * the arena has room for its fields, its inputs are copied in, and admitted
+ * requests are batched into one persistent kernel launch (a captured CUDA
+ * graph per launch slot) whose CTAs pull tiles of every request in the
+ * batch.  Up to `slots` launches are in flight on their own streams, so
+ * requests that arrive while others run are admitted and overlap with them.
+ * Requests too large to gain from batching run on their own plan on the
+ * same streams.  Every route computes each output with the reference's
+ * per-output FP32 order, so a result is bit-identical alone and in a mix.
+ *
+ * Convolution requests: FP32, BorderZero, no sampling, odd square filters up
+ * to 9x9 in the batch kernel (other descriptors run on their own plan);
+ * PLANE_BY_PLANE or PROJECT_FRAME_BLOCK_REDUCE_SUM with batch_size 1.
+ * Host pointers must stay valid until the request completes; pinned host
+ * memory (cct_host_alloc) gives full copy bandwidth.
+ * flags CCT_SERVE_PER_CALL: no batching; each request alone, in arrival
+ * order, through its plan with a synchronise per request (the plain
+ * per-call dispatch that serving is compared with). */
+enum { CCT_SERVE_CONV = 0, CCT_SERVE_GRAPH_STEP = 1 };
+enum { CCT_SERVE_PER_CALL = 0x1 };
+typedef struct cct_server_config {
+  int32_t struct_size;  /* sizeof(cct_server_config) */
+  int32_t slots;        /* launches in flight (1..8; 0 = 3) */
+  int32_t max_batch;    /* requests per launch (1..256; 0 = 64) */
+  int32_t flags;
+  uint64_t arena_bytes; /* HBM reserved for admitted requests (0 = 8 GiB) */
+} cct_server_config;
+typedef struct cct_serve_request {
+  int32_t struct_size;  /* sizeof(cct_serve_request) */
+  int32_t kind;         /* CCT_SERVE_CONV or CCT_SERVE_GRAPH_STEP */
+  cct_conv_desc desc;   /* CCT_SERVE_CONV */
+  const float *image;   /* host input (the graph's input field for a step) */
+  const float *filter;  /* host filter, or NULL for resident filter filter_id */
+  int32_t filter_id;
+  int32_t reserved;
+  float *out;           /* host output (the graph's last field for a step) */
+  cct_graph *graph;     /* CCT_SERVE_GRAPH_STEP */
+} cct_serve_request;
+typedef struct cct_server cct_server;
+void cct_server_config_init(cct_server_config *cfg);
+void cct_serve_request_init(cct_serve_request *req);
+int cct_server_create(const cct_server_config *cfg, cct_server **out);
+/* Waits for every submitted request, then stops the scheduler. */
+int cct_server_destroy(cct_server *server);
+/* A filter bank kept resident on the device; requests name it by id. */
+int cct_server_add_filter(cct_server *server, const float *host_filter, size_t elems, int32_t *id);
+/* Queues a request (CCT_EINVAL if it can never fit the arena or is malformed). */
+int cct_server_submit(cct_server *server, const cct_serve_request *req, uint64_t *ticket);
+/* CCT_OK once the request's output is in host memory; CCT_ETIMEOUT after
+ * timeout_ms (< 0: no limit); the request's own error status otherwise.
+ * latency_us (may be NULL): submit to completion, as seen by the scheduler. */
+int cct_server_wait(cct_server *server, uint64_t ticket, int32_t timeout_ms, double *latency_us);
+/* Open-loop replay: submits req[i] at arrival_s[i] seconds after the call
+ * (a client thread), waits for all, and writes each latency in µs.
+ * Returns the first error status, or CCT_OK. */
+int cct_server_replay(cct_server *server, const cct_serve_request *reqs, const double *arrival_s,
+                      int32_t n, double *latency_us);
+/* Counters since creation: requests completed, persistent launches, requests
+ * that ran on their own plan, peak arena bytes in use. */
+int cct_server_stats(const cct_server *server, uint64_t *completed, uint64_t *batches,
+                     uint64_t *solo, uint64_t *peak_arena_bytes);
+/* Page-locked host memory for request buffers. */
+int cct_host_alloc(void **ptr, size_t bytes);
+int cct_host_free(void *ptr);
 
 /* ---- device memory helpers (the JNI side has no CUDA runtime) ----------- */
 int cct_malloc(void **ptr, size_t bytes);

@@ -46,7 +46,7 @@ int oracle_output_shape(const oracle_desc *d, int *out_rows, int *out_cols,
   if (d->orient != OR_XCORR && d->orient != OR_CONV) ERR("bad orientation");
   if (sampling < OR_NOSAMPLE || sampling > OR_UP) ERR("bad sampling policy");
   if (sampling != OR_NOSAMPLE && d->step < 1) ERR("sampling step must be >= 1");
-  if (d->mode < OR_PLANE || d->mode > OR_BACKPROJECT_REDUCE) ERR("bad vector mode");
+  if (d->mode < OR_PLANE || d->mode > OR_FILTER_ADJOINT_REDUCE) ERR("bad vector mode");
   int step = sampling == OR_NOSAMPLE ? 1 : d->step;
   /* DynamicConvolutionGenerator.scala:497-505: odd filters for centred borders. */
   if (d->border != OR_VALID && d->border != OR_FULL &&
@@ -64,12 +64,15 @@ int oracle_output_shape(const oracle_desc *d, int *out_rows, int *out_cols,
   if (sampling == OR_UP && d->border == OR_CLAMP)
     ERR("integrated upsampling with BorderClamp convolution not supported");
 
-  /* ConvolveHyperKernel.outputFieldType :1306-1347 */
+  /* ConvolveHyperKernel.outputFieldType :1306-1347; FilterAdjoint upsamples
+   * the second operand instead of the input (:1313-1326). */
+  int fa = d->mode == OR_FILTER_ADJOINT || d->mode == OR_FILTER_ADJOINT_REDUCE;
+  int fup = (fa && sampling == OR_UP) ? step : 1;
   int ur = d->rows, uc = d->cols;
-  if (sampling == OR_UP) { ur *= step; uc *= step; }
+  if (sampling == OR_UP && !fa) { ur *= step; uc *= step; }
   int br = ur, bc = uc;
-  if (d->border == OR_VALID) { br = ur - d->f_rows + 1; bc = uc - d->f_cols + 1; }
-  if (d->border == OR_FULL) { br = ur + d->f_rows - 1; bc = uc + d->f_cols - 1; }
+  if (d->border == OR_VALID) { br = ur - d->f_rows * fup + 1; bc = uc - d->f_cols * fup + 1; }
+  if (d->border == OR_FULL) { br = ur + d->f_rows * fup - 1; bc = uc + d->f_cols * fup - 1; }
   if (br < 1 || bc < 1) ERR("BorderValid filter larger than the input");
   if (sampling == OR_DOWN) { br = (br + step - 1) / step; bc = (bc + step - 1) / step; }
 
@@ -81,6 +84,11 @@ int oracle_output_shape(const oracle_desc *d, int *out_rows, int *out_cols,
     if (!(d->planes <= 0 || d->f_planes <= 0 || d->planes == d->f_planes))
       ERR("plane-by-plane convolution needs a scalar operand or equal tensor shapes");
     oplanes = d->planes <= 0 ? pf : pin;
+  } else if (fa) {
+    /* :1366-1377 checks, :1414-1429 output planes */
+    if (pf % batch != 0) ERR("filter planes must be a multiple of the batch size");
+    if (pin % batch != 0) ERR("input planes must be a multiple of the batch size");
+    oplanes = (pin / batch) * (pf / batch) * (d->mode == OR_FILTER_ADJOINT ? batch : 1);
   } else {
     /* frameInputChecks :1349-1356 */
     if (pin % batch != 0) ERR("input planes must be a multiple of the batch size");
@@ -111,12 +119,17 @@ static plane_map make_map(const oracle_desc *d) {
   m.pf = plane_count(d->f_planes);
   m.batch = d->batch < 1 ? 1 : d->batch;
   m.n = m.pin / m.batch;
-  m.groups = m.pf / (m.n > 0 ? m.n : 1);
+  if (m.mode == OR_FILTER_ADJOINT || m.mode == OR_FILTER_ADJOINT_REDUCE)
+    m.groups = m.pf / m.batch;  /* gradient planes per image */
+  else
+    m.groups = m.pf / (m.n > 0 ? m.n : 1);
   return m;
 }
 
 static int map_terms(const plane_map *m, int o) {
+  (void)o;
   if (m->mode == OR_PROJECT_REDUCE || m->mode == OR_BACKPROJECT_REDUCE) return m->n;
+  if (m->mode == OR_FILTER_ADJOINT_REDUCE) return m->batch;
   return 1;
 }
 
@@ -144,10 +157,21 @@ static void map_pair(const plane_map *m, int o, int t, int *ip, int *fp) {
       *fp = m->groups * (w % m->n) + w / m->n;
       break;
     }
-    default: {                       /* out b*L+l = sum_n x[b*N+n] (*) f[n*L+l] */
+    case OR_BACKPROJECT_REDUCE: {    /* out b*L+l = sum_n x[b*N+n] (*) f[n*L+l] */
       int b = o / m->groups, l = o % m->groups;
       *ip = b * m->n + t;
       *fp = t * m->groups + l;
+      break;
+    }
+    case OR_FILTER_ADJOINT: {        /* out B*w+b = x[b*C + w%C] (*) g[b*L + w/C] (:187, 333, 575-590) */
+      int b = o % m->batch, w = o / m->batch;
+      *ip = b * m->n + w % m->n;
+      *fp = b * m->groups + w / m->n;
+      break;
+    }
+    default: {                       /* out w = sum_b x[b*C + w%C] (*) g[b*L + w/C] */
+      *ip = t * m->n + o % m->n;
+      *fp = t * m->groups + o / m->n;
       break;
     }
   }
@@ -192,11 +216,16 @@ static inline int div_floor(int a, int b) {
     int sampling = eff_sampling(d);                                            \
     int step = sampling == OR_NOSAMPLE ? 1 : d->step;                          \
     int down = sampling == OR_DOWN ? step : 1;                                 \
-    int up = sampling == OR_UP ? step : 1;                                     \
-    int hr = low_halo(d->border, d->f_rows), hc = low_halo(d->border, d->f_cols); \
-    int R = d->f_rows, S = d->f_cols, H = d->rows, W = d->cols;                \
+    /* FilterAdjoint upsamples the gradient (taps at multiples of fup), the \
+     * other modes the input (:1313-1326) */                                  \
+    int fa = d->mode == OR_FILTER_ADJOINT || d->mode == OR_FILTER_ADJOINT_REDUCE; \
+    int up = (sampling == OR_UP && !fa) ? step : 1;                            \
+    int fup = (sampling == OR_UP && fa) ? step : 1;                            \
+    int FR = d->f_rows, FS = d->f_cols;                                        \
+    int R = FR * fup, S = FS * fup, H = d->rows, W = d->cols;                  \
+    int hr = low_halo(d->border, R), hc = low_halo(d->border, S);              \
     int terms = map_terms(&m, o);                                              \
-    size_t page = (size_t)H * W, fpage = (size_t)R * S;                        \
+    size_t page = (size_t)H * W, fpage = (size_t)FR * FS;                      \
     for (int i = i0; i < i1; i++) {                                            \
       for (int jj = 0; jj < j->ocols; jj++) {                                  \
         T acc = 0;                                                             \
@@ -213,13 +242,15 @@ static inline int div_floor(int a, int b) {
             if (up > 1 && ((pr % up) + up) % up != 0) continue; /* :429 */     \
             int sr = border_index(d->border, up > 1 ? div_floor(pr, up) : pr, H); \
             T colSum = 0;                                                      \
+            int er = d->orient == OR_CONV ? R - 1 - r : r;                     \
             for (int s = 0; s < S; s++) {                                      \
               int pc = pc0 + s;                                                \
               if (up > 1 && ((pc % up) + up) % up != 0) continue;              \
               int sc = border_index(d->border, up > 1 ? div_floor(pc, up) : pc, W); \
               T v = (sr < 0 || sc < 0) ? (T)0 : xp[(size_t)sr * W + sc];       \
-              T w = d->orient == OR_CONV ? fpp[(size_t)(R - 1 - r) * S + (S - 1 - s)] \
-                                         : fpp[(size_t)r * S + s];             \
+              int es = d->orient == OR_CONV ? S - 1 - s : s;                   \
+              T w = (er % fup == 0 && es % fup == 0)                           \
+                        ? fpp[(size_t)(er / fup) * FS + es / fup] : (T)0;      \
               colSum = FMA(v, w, colSum);                                      \
             }                                                                  \
             rowSum = rowSum + colSum;                                          \

@@ -28,7 +28,8 @@ enum { OR_ZERO = 0, OR_CLAMP = 1, OR_CYCLIC = 2, OR_VALID = 3, OR_FULL = 4 };
 enum { OR_XCORR = 0, OR_CONV = 1 };
 enum { OR_NOSAMPLE = 0, OR_DOWN = 1, OR_UP = 2 };
 enum { OR_PLANE = 0, OR_PROJECT = 1, OR_PROJECT_REDUCE = 2,
-       OR_BACKPROJECT = 3, OR_BACKPROJECT_REDUCE = 4 };
+       OR_BACKPROJECT = 3, OR_BACKPROJECT_REDUCE = 4,
+       OR_FILTER_ADJOINT = 5, OR_FILTER_ADJOINT_REDUCE = 6 };
 
 typedef struct {
   int rows, cols;          /* input field shape (rows = 1 for a 1-D field)   */

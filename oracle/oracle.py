@@ -24,7 +24,7 @@ _LIB = None
 ZERO, CLAMP, CYCLIC, VALID, FULL = range(5)
 XCORR, CONV = 0, 1
 NOSAMPLE, DOWN, UP = 0, 1, 2
-PLANE, PROJECT, PROJECT_REDUCE, BACKPROJECT, BACKPROJECT_REDUCE = range(5)
+PLANE, PROJECT, PROJECT_REDUCE, BACKPROJECT, BACKPROJECT_REDUCE, FILTER_ADJOINT, FILTER_ADJOINT_REDUCE = range(7)
 
 
 class OracleDesc(ctypes.Structure):

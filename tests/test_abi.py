@@ -106,3 +106,41 @@ def test_plan_without_gpu_is_enodev():
     with pytest.raises(_lib.CctError) as e:
         _lib.Plan(d)
     assert e.value.status == _lib.ENODEV
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """ctypes mirrors of the ABI structs have the C compiler's sizes and offsets."""
+    import subprocess
+    src = tmp_path / "layout.c"
+    inc = Path(__file__).resolve().parent.parent / "include"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "cct_conv.h"\n'
+        "int main(void) {\n"
+        '  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(cct_conv_desc), sizeof(cct_server_config),\n'
+        "         sizeof(cct_serve_request), offsetof(cct_serve_request, image),\n"
+        "         offsetof(cct_serve_request, filter_id), offsetof(cct_serve_request, out),\n"
+        "         offsetof(cct_serve_request, graph));\n  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(inc), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    R = _lib.ServeRequest
+    assert got == [ctypes.sizeof(_lib.ConvDesc), ctypes.sizeof(_lib.ServerConfig), ctypes.sizeof(R),
+                   R.image.offset, R.filter_id.offset, R.out.offset, R.graph.offset]
+
+
+def test_server_and_graph_need_a_device():
+    cfg = _lib.ServerConfig()
+    _lib.LIB.cct_server_config_init(ctypes.byref(cfg))
+    assert cfg.struct_size == ctypes.sizeof(_lib.ServerConfig)
+    assert cfg.slots == 3 and cfg.max_batch == 64 and cfg.arena_bytes == 8 << 30
+    h = ctypes.c_void_p()
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    assert _lib.LIB.cct_server_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.ENODEV
+    bad = _lib.ServerConfig()
+    _lib.LIB.cct_server_config_init(ctypes.byref(bad))
+    bad.slots = 9
+    rc = _lib.LIB.cct_server_create(ctypes.byref(bad), ctypes.byref(h))
+    assert rc in (_lib.EINVAL, _lib.ENODEV)

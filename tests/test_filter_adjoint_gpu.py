@@ -1,0 +1,81 @@
+"""FilterAdjoint (weight-gradient plane mixing) on the GPU against the FP32
+oracle, bit for bit, and through the reference-named API."""
+import numpy as np
+import pytest
+import torch
+
+import cctconv as C
+import oracle as O
+from cctconv import _lib
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # planes per image C, gradient planes per image L, image rows, cols, gradient rows, cols, batch,
+    # border, sampling, step
+    (3, 4, 71, 23, 65, 17, 1, O.VALID, O.NOSAMPLE, 1),
+    (2, 3, 63, 67, 47, 51, 2, O.VALID, O.NOSAMPLE, 1),
+    (3, 4, 15, 27, 11, 23, 3, O.VALID, O.NOSAMPLE, 1),
+    (1, 4, 15, 27, 11, 23, 7, O.VALID, O.NOSAMPLE, 1),
+    (4, 2, 36, 36, 16, 16, 2, O.VALID, O.UP, 2),
+    (2, 2, 35, 35, 10, 10, 1, O.VALID, O.UP, 3),
+    (2, 3, 27, 27, 16, 16, 2, O.VALID, O.DOWN, 2),
+    (2, 2, 20, 24, 5, 7, 2, O.ZERO, O.NOSAMPLE, 1),
+    (2, 2, 20, 24, 5, 5, 2, O.FULL, O.NOSAMPLE, 1),
+    (32, 64, 68, 68, 64, 64, 2, O.VALID, O.NOSAMPLE, 1),  # a 5x5 filter gradient of a 64x64 layer
+]
+
+
+def _run(desc, x, g):
+    plan = _lib.Plan(desc)
+    orows, ocols, oplanes = plan.shape
+    y = torch.full((max(oplanes, 1), orows, ocols), float("nan"), device="cuda")
+    xd, gd = torch.from_numpy(x).cuda(), torch.from_numpy(g).cuda()  # kept alive across the run
+    plan.run(xd.data_ptr(), gd.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    plan.close()
+    return y.cpu().numpy()
+
+
+@pytest.mark.parametrize("mode", [O.FILTER_ADJOINT, O.FILTER_ADJOINT_REDUCE], ids=["fa", "fa_reduce"])
+@pytest.mark.parametrize("orient", [O.XCORR, O.CONV], ids=["xcorr", "conv"])
+@pytest.mark.parametrize("case", CASES, ids=lambda c: "-".join(map(str, c)))
+def test_filter_adjoint_matches_oracle_bitwise(case, orient, mode):
+    Cn, L, rows, cols, gr, gc, batch, border, sampling, step = case
+    rng = np.random.default_rng(rows * 31 + gr)
+    x = rng.uniform(-1, 1, (batch * Cn, rows, cols)).astype(np.float32)
+    g = rng.uniform(-1, 1, (batch * L, gr, gc)).astype(np.float32)
+    desc = _lib.new_desc(image_rows=rows, image_cols=cols, image_planes=batch * Cn, filter_rows=gr,
+                         filter_cols=gc, filter_planes=batch * L, batch_size=batch, border=border,
+                         orientation=orient, sampling=sampling, step=step,
+                         vector_mode=_lib.FILTER_ADJOINT if mode == O.FILTER_ADJOINT
+                         else _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM)
+    y = _run(desc, x, g)
+    od = O.make_desc(rows, cols, gr, gc, planes=batch * Cn, f_planes=batch * L, batch=batch,
+                     border=border, orient=orient, sampling=sampling, step=step, mode=mode)
+    ref = O.conv(od, x, g, np.float32)
+    assert y.size == ref.size
+    assert np.array_equal(y.reshape(ref.shape).view(np.uint32), ref.view(np.uint32))
+
+
+def test_filter_adjoint_api_and_scalar_result():
+    """crossCorrelateFilterAdjoint of two ScalarFields is a ScalarField; the
+    vector form follows the reference's plane order."""
+    rng = np.random.default_rng(1)
+    x = torch.from_numpy(rng.uniform(-1, 1, (40, 40)).astype(np.float32)).cuda()
+    g = torch.from_numpy(rng.uniform(-1, 1, (36, 36)).astype(np.float32)).cuda()
+    y = C.crossCorrelateFilterAdjoint(x, g, C.BorderValid)
+    assert y.shape == (5, 5)
+    yc = C.convolveFilterAdjoint(x, g, C.BorderValid, C.UpsampleInputConvolution(1))
+    assert yc.shape == (5, 5)
+    xv = torch.from_numpy(rng.uniform(-1, 1, (2 * 3, 20, 20)).astype(np.float32)).cuda()
+    gv = torch.from_numpy(rng.uniform(-1, 1, (2 * 4, 16, 16)).astype(np.float32)).cuda()
+    fa = C.crossCorrelateFilterAdjoint(xv, gv, C.BorderValid, batchSize=2)
+    red = C.filterAdjointBlockReduceSum(xv, gv, C.BorderValid, batchSize=2)
+    assert fa.shape == (3 * 4 * 2, 5, 5) and red.shape == (12, 5, 5)
+    torch.cuda.synchronize()
+    # plane B*w + b of the unreduced form, summed over b in order, is the reduced form
+    acc = fa[0::2] + fa[1::2]
+    assert torch.equal(acc, red)
+    with pytest.raises(ValueError, match="multiple of the batchSize"):
+        C.crossCorrelateFilterAdjoint(xv, gv[:7], C.BorderValid, batchSize=2)

@@ -214,3 +214,112 @@ def test_fused_backproject_is_adjoint_of_projectframe():
 def test_poor_float_semantics():
     assert O.poor_float_equal([1.0, 0.0], [1.0 + 1e-4, 1e-3])
     assert not O.poor_float_equal([1.0], [1.01])
+
+
+# ---------------------------------------------------------------- FilterAdjoint
+def _fa(x, g, border=O.VALID, orient=O.CONV, sampling=O.NOSAMPLE, step=1, batch=1,
+        mode=O.FILTER_ADJOINT, dtype=np.float32, planes=None, g_planes=None):
+    x = np.asarray(x, dtype)
+    g = np.asarray(g, dtype)
+    rows, cols = x.shape[-2:]
+    d = O.make_desc(rows, cols, g.shape[-2], g.shape[-1],
+                    planes=x.shape[0] if planes is None else planes,
+                    f_planes=g.shape[0] if g_planes is None else g_planes,
+                    batch=batch, border=border, orient=orient, sampling=sampling, step=step, mode=mode)
+    return O.conv(d, x, g, dtype)
+
+
+@pytest.mark.parametrize("n_in,f_size,down", [(1 + 15, 16, 1), (5 + 15, 16, 1), (9 + 15, 16, 1),
+                                              (137, 128, 1), (27, 16, 2), (32, 24, 3)])
+def test_filter_adjoint_constant_known_answers(n_in, f_size, down):
+    """StaticConvolutionSpec.scala:992-1037: a constant 0.5 field and an all-ones
+    gradient give f_size^2 * 0.5 at every output."""
+    x = np.full((n_in, n_in), 0.5, np.float32)
+    g = np.ones((f_size, f_size), np.float32)
+    y = _fa(x[None], g[None], sampling=O.DOWN if down > 1 else O.NOSAMPLE, step=down,
+            planes=0, g_planes=0)
+    out = (n_in - f_size + 1) // down
+    assert y.shape[-2:] == (out, out)
+    assert np.all(y == f_size * f_size * 0.5)
+
+
+@pytest.mark.parametrize("orient", [O.CONV, O.XCORR])
+@pytest.mark.parametrize("n_in,f_size,up", [(137, 64, 2), (35, 10, 3), (210, 50, 4)])
+def test_filter_adjoint_upsampled_gradient_known_answers(orient, n_in, f_size, up):
+    """StaticConvolutionSpec.scala:1039-1147: UpsampleInput upsamples the
+    gradient; output side n - f*up + 1."""
+    x = np.full((n_in, n_in), 0.5, np.float32)
+    g = np.ones((f_size, f_size), np.float32)
+    y = _fa(x[None], g[None], orient=orient, sampling=O.UP, step=up, planes=0, g_planes=0)
+    out = n_in - f_size * up + 1
+    assert y.shape[-2:] == (out, out)
+    assert np.all(y == f_size * f_size * 0.5)
+
+
+@pytest.mark.parametrize("orient", [O.CONV, O.XCORR])
+def test_filter_adjoint_upsampled_sparse_input(orient):
+    """StaticConvolutionSpec.scala:1075-1097 / 1124-1146 (360, 50, 7)."""
+    n_in, f_size, up = 360, 50, 7
+    x = np.zeros((n_in, n_in), np.float32)
+    x[:up, :up] = 0.5
+    g = np.ones((f_size, f_size), np.float32)
+    y = _fa(x[None], g[None], orient=orient, sampling=O.UP, step=up, planes=0, g_planes=0).reshape(
+        n_in - f_size * up + 1, -1)
+    want = np.zeros_like(y)
+    if orient == O.CONV:
+        want[0, 0] = 0.5
+    else:
+        want[:up, :up] = 0.5
+    assert np.array_equal(y, want)
+
+
+@pytest.mark.parametrize("n", [2, 3, 5])
+def test_filter_adjoint_upsample_flip_order(n):
+    """StaticConvolutionSpec.scala:1152-1189: a 1x1 gradient upsampled by the
+    field size reads the first element (cross-correlation) or the last
+    (convolution)."""
+    x = (n * np.arange(n)[:, None] + np.arange(n)[None, :] + 1).astype(np.float32)
+    g = np.ones((1, 1), np.float32)
+    yc = _fa(x[None], g[None], orient=O.CONV, sampling=O.UP, step=n, planes=0, g_planes=0)
+    yx = _fa(x[None], g[None], orient=O.XCORR, sampling=O.UP, step=n, planes=0, g_planes=0)
+    assert yc.ravel().tolist() == [n * n] and yx.ravel().tolist() == [1.0]
+
+
+@pytest.mark.parametrize("C,L,rows,cols,out,batch", [(3, 4, 71, 23, 7, 1), (2, 2, 19, 17, 7, 1),
+                                                     (1, 4, 31, 23, 12, 1), (6, 1, 23, 29, 7, 1),
+                                                     (2, 3, 63, 67, 17, 2), (3, 4, 15, 27, 5, 3),
+                                                     (1, 4, 15, 27, 5, 7), (6, 1, 15, 27, 5, 8)])
+def test_filter_adjoint_plane_mixing_by_composition(C, L, rows, cols, out, batch):
+    """StaticConvolutionSpec.scala:1950-2050: output plane i (b = i % B,
+    w = i / B) is crossCorrelate(image[b*C + w%C], grad[b*L + w/C], BorderValid);
+    the block-reduced form sums the B images of w in order."""
+    rng = np.random.default_rng(C * 100 + L)
+    kr, kc = rows - out + 1, cols - out + 1
+    x = rng.uniform(-1, 1, (batch * C, rows, cols)).astype(np.float32)
+    g = rng.uniform(-1, 1, (batch * L, kr, kc)).astype(np.float32)
+    y = _fa(x, g, orient=O.XCORR, batch=batch).reshape(C * L * batch, out, -1)
+    for i in range(C * L * batch):
+        b, w = i % batch, i // batch
+        want = _fa(x[b * C + w % C][None], g[b * L + w // C][None], orient=O.XCORR, planes=0,
+                   g_planes=0, mode=O.PLANE)
+        assert np.array_equal(y[i], want.reshape(y[i].shape)), i
+    y64 = _fa(x, g, orient=O.XCORR, batch=batch, dtype=np.float64).reshape(C * L * batch, out, -1)
+    r64 = _fa(x, g, orient=O.XCORR, batch=batch, dtype=np.float64,
+              mode=O.FILTER_ADJOINT_REDUCE).reshape(C * L, out, -1)
+    for w in range(C * L):
+        acc = np.zeros_like(r64[w])
+        for b in range(batch):
+            acc = acc + y64[w * batch + b]
+        assert np.array_equal(acc, r64[w])
+
+
+def test_filter_adjoint_shape_rules():
+    def shape(mode, planes, f_planes, batch, sampling=O.NOSAMPLE, step=1):
+        return O.output_shape(O.make_desc(40, 40, 8, 8, planes=planes, f_planes=f_planes, batch=batch,
+                                          border=O.VALID, orient=O.XCORR, sampling=sampling,
+                                          step=step, mode=mode))
+    assert shape(O.FILTER_ADJOINT, 6, 8, 2) == (33, 33, 3 * 4 * 2)
+    assert shape(O.FILTER_ADJOINT_REDUCE, 6, 8, 2) == (33, 33, 12)
+    assert shape(O.FILTER_ADJOINT, 6, 8, 2, O.UP, 2) == (40 - 16 + 1, 25, 24)
+    with pytest.raises(ValueError):
+        shape(O.FILTER_ADJOINT, 6, 7, 2)

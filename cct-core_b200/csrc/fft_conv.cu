@@ -10,16 +10,21 @@
 // at the origin with cyclic wrap-around.  This equals the direct convolution
 // with the same border policy at every output point.
 //
-// Three kernels per run, each a shared-memory radix-4 Stockham FFT:
-//   fft_rows_r2c   one expanded row per CTA: Fc reals packed as Fc/2 complex,
-//                  N = Fc/2 point FFT, then the even/odd split to the
-//                  Fc/2 + 1 non-negative frequencies;
-//   fft_cols       a block of spectrum columns per CTA: Fr-point FFT down
-//                  each column, times G, inverse FFT (or, for a dynamic
-//                  filter's spectrum, forward FFT and scaling only);
-//   fft_rows_c2r   one output row per CTA: inverse of the split, N-point
-//                  inverse FFT, unpacked and trimmed to the field.
-// Twiddles are computed in FP64 on the host and stored as float2.
+// Three kernels per run:
+//   fft_rows_r2c   expanded rows (Fc reals packed as N = Fc/2 complex): N-point
+//                  FFT, then the even/odd split to the Fc/2 + 1 non-negative
+//                  frequencies;
+//   fft_cols       blocks of spectrum columns: Fr-point FFT down each
+//                  column, times G, inverse FFT (or, for a dynamic filter's
+//                  spectrum, forward FFT and scaling only);
+//   fft_rows_c2r   output rows: inverse of the split, N-point inverse FFT,
+//                  unpacked and trimmed to the field.
+// Each FFT is a Stockham autosort in radix-16 passes (radix 2/4/8 for the
+// last): every thread keeps 16 complex values in registers and does one
+// 16-point (or 16/R R-point) DFT per pass, so an N-point FFT takes
+// ceil(log2 N / 4) shared-memory exchanges.  Shared-memory sequences are
+// padded by one element every 16 so the strided exchanges stay free of bank
+// conflicts.  Twiddles are computed in FP64 on the host and stored as float2.
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -31,7 +36,8 @@
 namespace cct {
 namespace {
 
-constexpr int kFftThreads = 256;
+constexpr int kRowThreads = 256;
+constexpr int kColThreads = 512;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -39,66 +45,170 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
-// `cols` independent N-point DFTs (N = 2^logN) of the sequences a[c*N .. c*N+N)
-// in shared memory, Stockham autosort with radix-4 stages (and one radix-2
-// stage when logN is odd), ping-ponging with b.  tw[k] = exp(-2 pi i k / N).
-// inverse: exp(+...) and no scaling.  Returns the buffer holding the result.
-__device__ float2 *stockham(float2 *a, float2 *b, int N, int logN, int cols,
-                            const float2 *__restrict__ tw, bool inverse) {
-  int Ns = 1;
-  for (int st = 0; st < logN / 2; ++st) {
-    const int q = N / 4, tstep = N / (4 * Ns);
-    for (int t = threadIdx.x; t < q * cols; t += blockDim.x) {
-      const int c = t / q, j = t - c * q;
-      const float2 *src = a + c * N;
-      float2 *dst = b + c * N;
-      const int k = j & (Ns - 1);
-      float2 w1 = __ldg(tw + k * tstep), w2 = __ldg(tw + 2 * k * tstep), w3 = __ldg(tw + 3 * k * tstep);
-      if (inverse) {
-        w1 = conjf2(w1);
-        w2 = conjf2(w2);
-        w3 = conjf2(w3);
+// multiply by -i (forward transform) or +i (inverse)
+template <bool INV>
+__device__ __forceinline__ float2 rot(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// multiply by exp(-+ 2 pi i j / 16): forward uses the minus sign
+template <bool INV>
+__device__ __forceinline__ float2 w16(float2 a, float c, float s) {
+  return cmul(a, make_float2(c, INV ? s : -s));
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft2(float2 *v) {
+  const float2 a = v[0];
+  v[0] = cadd(a, v[1]);
+  v[1] = csub(a, v[1]);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2 &a0, float2 &a1, float2 &a2, float2 &a3) {
+  const float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = rot<INV>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft8(float2 *v) {
+  constexpr float h = 0.70710678118654752f;  // cos(pi/4)
+  float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<INV>(e0, e1, e2, e3);
+  dft4<INV>(o0, o1, o2, o3);
+  o1 = w16<INV>(o1, h, h);   // W8^1
+  o2 = rot<INV>(o2);         // W8^2
+  o3 = w16<INV>(o3, -h, h);  // W8^3
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft16(float2 *v) {
+  constexpr float c1 = 0.92387953251128674f, s1 = 0.38268343236508978f;  // cos, sin(pi/8)
+  constexpr float h = 0.70710678118654752f;
+  // n = 4p + q: 4-point DFTs over p, twiddles W16^(q k1), 4-point DFTs over q
+#pragma unroll
+  for (int q = 0; q < 4; ++q) dft4<INV>(v[q], v[q + 4], v[q + 8], v[q + 12]);
+  v[5] = w16<INV>(v[5], c1, s1);     // q=1 k1=1
+  v[9] = w16<INV>(v[9], h, h);       // q=1 k1=2
+  v[13] = w16<INV>(v[13], s1, c1);   // q=1 k1=3
+  v[6] = w16<INV>(v[6], h, h);       // q=2 k1=1
+  v[10] = rot<INV>(v[10]);           // q=2 k1=2
+  v[14] = w16<INV>(v[14], -h, h);    // q=2 k1=3
+  v[7] = w16<INV>(v[7], s1, c1);     // q=3 k1=1
+  v[11] = w16<INV>(v[11], -h, h);    // q=3 k1=2
+  v[15] = w16<INV>(v[15], -c1, -s1); // q=3 k1=3 (W16^9)
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4<INV>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+  // X[k1 + 4 k2] sits in v[4 k1 + k2]: transpose to natural order
+  float2 t[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) t[m] = v[4 * (m & 3) + (m >> 2)];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) v[m] = t[m];
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 *v) {
+  if (R == 2) dft2<INV>(v);
+  if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+  if (R == 8) dft8<INV>(v);
+  if (R == 16) dft16<INV>(v);
+}
+
+// One Stockham pass of radix R over an N-point sequence (T = N/16 threads,
+// thread tt owns butterflies j = tt + q*T, q < 16/R): twiddles
+// w_(Ns R)^(m k) on input m (k = j mod Ns), then the R-point DFT.
+template <int R, bool INV>
+__device__ __forceinline__ void pass_compute(float2 (&v)[16], int N, int Ns, int T, int tt,
+                                             const float2 *__restrict__ tw) {
+#pragma unroll
+  for (int q = 0; q < 16 / R; ++q) {
+    const int j = tt + q * T, k = j & (Ns - 1);
+    if (k) {
+      const int step = N / (Ns * R);
+#pragma unroll
+      for (int m = 1; m < R; ++m) {
+        const float2 w = __ldg(tw + m * k * step);
+        v[q * R + m] = cmul(v[q * R + m], INV ? conjf2(w) : w);
       }
-      const float2 v0 = src[j];
-      const float2 v1 = cmul(src[j + q], w1);
-      const float2 v2 = cmul(src[j + 2 * q], w2);
-      const float2 v3 = cmul(src[j + 3 * q], w3);
-      const float2 t0 = cadd(v0, v2), t1 = csub(v0, v2), t2 = cadd(v1, v3), d = csub(v1, v3);
-      // forward: t3 = -i*d ; inverse: t3 = +i*d
-      const float2 t3 = inverse ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
-      const int base = (j - k) * 4 + k;
-      dst[base] = cadd(t0, t2);
-      dst[base + Ns] = cadd(t1, t3);
-      dst[base + 2 * Ns] = csub(t0, t2);
-      dst[base + 3 * Ns] = csub(t1, t3);
+    }
+    dft<R, INV>(v + q * R);
+  }
+}
+
+template <int R>
+__device__ __forceinline__ void pass_load(const float2 *s, float2 (&v)[16], int N, int T, int tt) {
+#pragma unroll
+  for (int q = 0; q < 16 / R; ++q)
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[q * R + m] = s[pad16(tt + q * T + m * (N / R))];
+}
+
+template <int R>
+__device__ __forceinline__ void pass_store(float2 *s, const float2 (&v)[16], int Ns, int T, int tt) {
+#pragma unroll
+  for (int q = 0; q < 16 / R; ++q) {
+    const int j = tt + q * T, k = j & (Ns - 1), base = (j - k) * R + k;
+#pragma unroll
+    for (int m = 0; m < R; ++m) s[pad16(base + m * Ns)] = v[q * R + m];
+  }
+}
+
+// N-point FFT (N = 2^logN >= 16) of the sequence whose first-pass inputs
+// v[m] = x[tt + m*T] the caller loaded; the result lands in natural order in
+// s (padded).  Every thread of the CTA calls this with the same N.
+template <bool INV>
+__device__ void fft_seq(float2 *s, float2 (&v)[16], int N, int logN, int T, int tt,
+                        const float2 *__restrict__ tw) {
+  int Ns = 1, rem = logN;
+  bool first = true;
+  while (rem > 0) {
+    const int b = rem >= 4 ? 4 : rem;
+    switch (b) {
+      case 4:
+        if (!first) pass_load<16>(s, v, N, T, tt);
+        pass_compute<16, INV>(v, N, Ns, T, tt, tw);
+        __syncthreads();
+        pass_store<16>(s, v, Ns, T, tt);
+        break;
+      case 3:
+        if (!first) pass_load<8>(s, v, N, T, tt);
+        pass_compute<8, INV>(v, N, Ns, T, tt, tw);
+        __syncthreads();
+        pass_store<8>(s, v, Ns, T, tt);
+        break;
+      case 2:
+        if (!first) pass_load<4>(s, v, N, T, tt);
+        pass_compute<4, INV>(v, N, Ns, T, tt, tw);
+        __syncthreads();
+        pass_store<4>(s, v, Ns, T, tt);
+        break;
+      default:
+        if (!first) pass_load<2>(s, v, N, T, tt);
+        pass_compute<2, INV>(v, N, Ns, T, tt, tw);
+        __syncthreads();
+        pass_store<2>(s, v, Ns, T, tt);
+        break;
     }
     __syncthreads();
-    float2 *tmp = a;
-    a = b;
-    b = tmp;
-    Ns *= 4;
+    Ns <<= b;
+    rem -= b;
+    first = false;
   }
-  if (logN & 1) {
-    const int h = N / 2, tstep = N / (2 * Ns);
-    for (int t = threadIdx.x; t < h * cols; t += blockDim.x) {
-      const int c = t / h, j = t - c * h;
-      const float2 *src = a + c * N;
-      float2 *dst = b + c * N;
-      const int k = j & (Ns - 1);
-      float2 w = __ldg(tw + k * tstep);
-      if (inverse) w = conjf2(w);
-      const float2 v0 = src[j], v1 = cmul(src[j + h], w);
-      const int base = (j - k) * 2 + k;
-      dst[base] = cadd(v0, v1);
-      dst[base + Ns] = csub(v0, v1);
-    }
-    __syncthreads();
-    float2 *tmp = a;
-    a = b;
-    b = tmp;
-  }
-  return a;
 }
 
 // Expanded-grid coordinate -> field coordinate (or -1 = zero): positions past
@@ -110,63 +220,74 @@ __device__ __forceinline__ int expand_index(int p, int n, int F, int border) {
   return border_index(border, v, n);
 }
 
-// Row pass: one expanded row (image) or one filter row per CTA -> half spectrum.
-// SRC 0: image plane `plane` of x expanded with the border; 1: filter plane
-// `plane` centred at the origin (flipped for convolution).
+// Filter tap landing on expanded coordinate `pos` (or -1): g[(r - h) mod F]
+// = f[r] for convolution, g[(h - r) mod F] = f[r] for cross-correlation.
+__device__ __forceinline__ int filter_index(int pos, int h, int R, int F, bool conv) {
+  int r = conv ? pos + h : h - pos;
+  if (conv) {
+    if (r >= F) r -= F;
+  } else {
+    if (r < 0) r += F;
+  }
+  return (r >= 0 && r < R) ? r : -1;
+}
+
+// Row pass: rows_per_cta sequences of N = Fc/2 complex points per CTA.
+// SRC 0: image plane rows expanded with the border; 1: filter plane rows
+// centred at the origin (flipped for convolution).
 template <int SRC>
-__global__ void __launch_bounds__(kFftThreads)
+__global__ void __launch_bounds__(kRowThreads)
     fft_rows_r2c(FftParams p, const float *__restrict__ src, float2 *__restrict__ spec, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int N = p.Fc / 2;
-  float2 *a = fsm, *b = fsm + N;
-  const int row = blockIdx.x % p.Fr, pl = blockIdx.x / p.Fr;
-  if (pl >= planes) return;
+  const int N = p.Fc / 2, T = N / 16, per = blockDim.x / T;
+  const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
+  const int gr = blockIdx.x * per + sub;
+  const bool active = gr < planes * p.Fr;
+  const int row = gr % p.Fr, pl = gr / p.Fr;
+  float2 *s = fsm + sub * (N + N / 16);
   const ConvGeom &g = p.g;
+  float2 v[16];
   if (SRC == 0) {
-    int ip, fp;
-    plane_pair(g, pl, 0, &ip, &fp);
+    int ip = 0, fp;
+    if (active) plane_pair(g, pl, 0, &ip, &fp);
     const float *xp = src + (size_t)ip * g.H * g.W;
-    const int sr = expand_index(row, g.H, p.Fr, g.border);
-    for (int n = threadIdx.x; n < N; n += blockDim.x) {
-      float v[2];
-      for (int e = 0; e < 2; ++e) {
-        const int sc = expand_index(2 * n + e, g.W, p.Fc, g.border);
-        v[e] = (sr >= 0 && sc >= 0) ? __ldg(xp + (size_t)sr * g.W + sc) : 0.0f;
+    const int sr = active ? expand_index(row, g.H, p.Fr, g.border) : -1;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int n = tt + m * T;
+      float e[2];
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int sc = expand_index(2 * n + k, g.W, p.Fc, g.border);
+        e[k] = (sr >= 0 && sc >= 0) ? __ldg(xp + (size_t)sr * g.W + sc) : 0.0f;
       }
-      a[n] = make_float2(v[0], v[1]);
+      v[m] = make_float2(e[0], e[1]);
     }
   } else {
-    // g[(r - h) mod Fr][(s - h) mod Fc] = f[r][s] for convolution,
-    // g[(h - r) mod Fr][(h - s) mod Fc] = f[r][s] for cross-correlation.
     const float *fp = src + (size_t)pl * g.R * g.S;
-    const int hr = (g.R - 1) / 2, hc = (g.S - 1) / 2;
     const bool conv = g.orient == CCT_CONVOLUTION;
-    // filter row r landing on this expanded row
-    int r = conv ? row + hr : hr - row;
-    if (conv) { if (r >= p.Fr) r -= p.Fr; } else { if (r < 0) r += p.Fr; }
-    // rows far from the origin are empty; so are filter rows that do not exist
-    const bool has = r >= 0 && r < g.R && ((conv ? (r - hr) : (hr - r)) % p.Fr + p.Fr) % p.Fr == row;
-    for (int n = threadIdx.x; n < N; n += blockDim.x) {
-      float v[2] = {0.0f, 0.0f};
-      if (has) {
-        for (int e = 0; e < 2; ++e) {
-          const int col = 2 * n + e;
-          int s = conv ? col + hc : hc - col;
-          if (conv) { if (s >= p.Fc) s -= p.Fc; } else { if (s < 0) s += p.Fc; }
-          if (s >= 0 && s < g.S && ((conv ? (s - hc) : (hc - s)) % p.Fc + p.Fc) % p.Fc == col)
-            v[e] = __ldg(fp + (size_t)r * g.S + s);
+    const int r = active ? filter_index(row, (g.R - 1) / 2, g.R, p.Fr, conv) : -1;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int n = tt + m * T;
+      float e[2] = {0.0f, 0.0f};
+      if (r >= 0) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int c = filter_index(2 * n + k, (g.S - 1) / 2, g.S, p.Fc, conv);
+          if (c >= 0) e[k] = __ldg(fp + (size_t)r * g.S + c);
         }
       }
-      a[n] = make_float2(v[0], v[1]);
+      v[m] = make_float2(e[0], e[1]);
     }
   }
-  __syncthreads();
-  float2 *z = stockham(a, b, N, p.logN, 1, p.tw_n, false);
+  fft_seq<false>(s, v, N, p.logN, T, tt, p.tw_n);
+  if (!active) return;
   // X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i,
   // W = exp(-2 pi i / Fc), k = 0..N
   float2 *out = spec + ((size_t)pl * p.Fr + row) * p.ld;
-  for (int k = threadIdx.x; k <= N; k += blockDim.x) {
-    const float2 zk = z[k == N ? 0 : k], zn = conjf2(z[k == 0 ? 0 : N - k]);
+  for (int k = tt; k <= N; k += T) {
+    const float2 zk = s[pad16(k == N ? 0 : k)], zn = conjf2(s[pad16(k == 0 ? 0 : N - k)]);
     const float2 e = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y + zn.y));
     const float2 dd = make_float2(0.5f * (zk.x - zn.x), 0.5f * (zk.y - zn.y));
     const float2 o = make_float2(dd.y, -dd.x);  // dd / i
@@ -174,71 +295,85 @@ __global__ void __launch_bounds__(kFftThreads)
   }
 }
 
-// Column pass over CW spectrum columns per CTA.
-// MODE 0: forward FFT, times G[fplane], inverse FFT (in place in spec).
+// Column pass over blockDim/T spectrum columns per CTA (c fastest across
+// threads, so each warp reads 32-byte row segments).
+// MODE 0: forward FFT, times G[fplane], inverse FFT, in place in spec.
 // MODE 1: forward FFT and scaling by p.scale (a filter's spectrum).
-template <int MODE, int CW>
-__global__ void __launch_bounds__(kFftThreads)
+template <int MODE>
+__global__ void __launch_bounds__(kColThreads)
     fft_cols(FftParams p, float2 *__restrict__ spec, const float2 *__restrict__ G, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int Fr = p.Fr, ncol = p.Fc / 2 + 1;
+  const int Fr = p.Fr, T = Fr / 16, CW = blockDim.x / T, ncol = p.Fc / 2 + 1;
   const int cblocks = (ncol + CW - 1) / CW;
   const int pl = blockIdx.x / cblocks, c0 = (blockIdx.x - pl * cblocks) * CW;
-  if (pl >= planes) return;
-  float2 *a = fsm, *b = fsm + CW * Fr;
-  float2 *sp = spec + (size_t)pl * Fr * p.ld;
-  for (int t = threadIdx.x; t < CW * Fr; t += blockDim.x) {
-    const int r = t / CW, c = t - r * CW;
-    a[c * Fr + r] = (c0 + c < ncol) ? sp[(size_t)r * p.ld + c0 + c] : make_float2(0.0f, 0.0f);
-  }
-  __syncthreads();
-  float2 *z = stockham(a, b, Fr, p.logR, CW, p.tw_r, false);
+  const int c = threadIdx.x % CW, tt = threadIdx.x / CW, col = c0 + c;
+  const bool active = col < ncol;
+  float2 *s = fsm + c * (Fr + Fr / 16);
+  float2 *sp = spec + (size_t)pl * Fr * p.ld + col;
+  float2 v[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) v[m] = active ? sp[(size_t)(tt + m * T) * p.ld] : make_float2(0.0f, 0.0f);
+  fft_seq<false>(s, v, Fr, p.logR, T, tt, p.tw_r);
   if (MODE == 0) {
     int ip, fp;
     plane_pair(p.g, pl, 0, &ip, &fp);
-    const float2 *gp = G + (size_t)fp * Fr * p.ld;
-    for (int t = threadIdx.x; t < CW * Fr; t += blockDim.x) {
-      const int c = t / Fr, r = t - c * Fr;
-      if (c0 + c < ncol) z[t] = cmul(z[t], __ldg(gp + (size_t)r * p.ld + c0 + c));
+    const float2 *gp = G + (size_t)fp * Fr * p.ld + col;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int r = tt + m * T;
+      v[m] = active ? cmul(s[pad16(r)], __ldg(gp + (size_t)r * p.ld)) : make_float2(0.0f, 0.0f);
     }
-    __syncthreads();
-    float2 *other = (z == a) ? b : a;
-    z = stockham(z, other, Fr, p.logR, CW, p.tw_r, true);
+    fft_seq<true>(s, v, Fr, p.logR, T, tt, p.tw_r);
+    if (!active) return;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int r = tt + m * T;
+      sp[(size_t)r * p.ld] = s[pad16(r)];
+    }
   } else {
-    for (int t = threadIdx.x; t < CW * Fr; t += blockDim.x) z[t] = make_float2(z[t].x * p.scale, z[t].y * p.scale);
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < CW * Fr; t += blockDim.x) {
-    const int r = t / CW, c = t - r * CW;
-    if (c0 + c < ncol) sp[(size_t)r * p.ld + c0 + c] = z[c * Fr + r];
+    if (!active) return;
+#pragma unroll
+    for (int m = 0; m < 16; ++m) {
+      const int r = tt + m * T;
+      sp[(size_t)r * p.ld] = cscale(s[pad16(r)], p.scale);
+    }
   }
 }
 
-// Inverse row pass: half spectrum row -> real row, trimmed to the output.
-__global__ void __launch_bounds__(kFftThreads)
+// Inverse row pass: half-spectrum rows -> real rows, trimmed to the output.
+__global__ void __launch_bounds__(kRowThreads)
     fft_rows_c2r(FftParams p, const float2 *__restrict__ spec, float *__restrict__ y, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int N = p.Fc / 2;
-  float2 *a = fsm, *b = fsm + N;
   const ConvGeom &g = p.g;
-  const int row = blockIdx.x % g.OH, pl = blockIdx.x / g.OH;
-  if (pl >= planes) return;
+  const int N = p.Fc / 2, T = N / 16, per = blockDim.x / T;
+  const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
+  const int gr = blockIdx.x * per + sub;
+  const bool active = gr < planes * g.OH;
+  const int row = gr % g.OH, pl = gr / g.OH;
+  float2 *s = fsm + sub * (N + N / 16);
   const float2 *in = spec + ((size_t)pl * p.Fr + row) * p.ld;
   // Z[k] = E[k] + i O[k], E = (X[k] + conj X[N-k]) / 2, O = (X[k] - conj X[N-k]) / 2 * conj(W^k)
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
-    const float2 xk = __ldg(in + k), xn = conjf2(__ldg(in + N - k));
-    const float2 e = make_float2(0.5f * (xk.x + xn.x), 0.5f * (xk.y + xn.y));
-    const float2 dd = make_float2(0.5f * (xk.x - xn.x), 0.5f * (xk.y - xn.y));
-    const float2 o = cmul(dd, conjf2(__ldg(p.tw_2n + k)));
-    a[k] = make_float2(e.x - o.y, e.y + o.x);  // e + i*o
+  float2 v[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int k = tt + m * T;
+    float2 z = make_float2(0.0f, 0.0f);
+    if (active) {
+      const float2 xk = __ldg(in + k), xn = conjf2(__ldg(in + N - k));
+      const float2 e = make_float2(0.5f * (xk.x + xn.x), 0.5f * (xk.y + xn.y));
+      const float2 dd = make_float2(0.5f * (xk.x - xn.x), 0.5f * (xk.y - xn.y));
+      const float2 o = cmul(dd, conjf2(__ldg(p.tw_2n + k)));
+      z = make_float2(e.x - o.y, e.y + o.x);  // e + i*o
+    }
+    v[m] = z;
   }
-  __syncthreads();
-  const float2 *z = stockham(a, b, N, p.logN, 1, p.tw_n, true);
+  fft_seq<true>(s, v, N, p.logN, T, tt, p.tw_n);
+  if (!active) return;
   float *yr = y + ((size_t)pl * g.OH + row) * g.OW;
   const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
-  for (int j = threadIdx.x; j < g.OW; j += blockDim.x) {
-    const float2 v = z[j >> 1];
-    const float o = (j & 1) ? v.y : v.x;
+  for (int j = tt; j < g.OW; j += T) {
+    const float2 z = s[pad16(j >> 1)];
+    const float o = (j & 1) ? z.y : z.x;
     yr[j] = relu ? fmaxf(o, 0.0f) : o;
   }
 }
@@ -257,10 +392,6 @@ int set_smem(K kern, size_t bytes) {
                                          (int)bytes),
                     "cudaFuncSetAttribute(fft)");
 }
-
-// Spectrum columns per CTA in the column pass: 4, or 2 for 4096-point columns
-// (the ping-pong buffers hold 2 x cols x Fr complex values).
-int col_width(int Fr) { return Fr > 2048 ? 2 : 4; }
 
 // One-dimensional forward FFT of length n in FP64 (iterative radix-2, natural
 // order) of v[0], v[stride], ...; w[k] = exp(-2 pi i k / n), k < n/2.
@@ -312,8 +443,9 @@ bool fft_plan(const ConvGeom &g, FftParams *out) {
   };
   p.Fr = size(g.H, hr);
   p.Fc = size(g.W, hc);
-  if (p.Fc < 8) p.Fc = 8;
-  if (p.Fr < 4) p.Fr = 4;
+  // the register FFTs want at least 16 points per sequence
+  if (p.Fc < 32) p.Fc = 32;
+  if (p.Fr < 16) p.Fr = 16;
   if (p.Fr > 4096 || p.Fc > 8192) return false;
   if (g.R > p.Fr || g.S > p.Fc) return false;  // no tap may wrap onto another
   // the border extension must fit between the field and its wrapped copy
@@ -321,7 +453,7 @@ bool fft_plan(const ConvGeom &g, FftParams *out) {
     return false;
   p.logN = ilog2(p.Fc / 2);
   p.logR = ilog2(p.Fr);
-  p.ld = p.Fc / 2 + 1;
+  p.ld = ((p.Fc / 2 + 1) + 3) & ~3;  // 32-byte aligned spectrum rows
   p.scale = 1.0f / ((float)p.Fr * (float)(p.Fc / 2));
   p.spec_elems = (size_t)g.pout * p.Fr * p.ld;
   p.filter_elems = (size_t)g.pf * p.Fr * p.ld;
@@ -391,24 +523,34 @@ void fft_static_spectrum(const FftParams &p, const float *host_filter, std::vect
   }
 }
 
-template <int MODE, int CW>
+template <int MODE>
 int launch_cols(const FftParams &p, float2 *spec, const float2 *G, int planes, cudaStream_t st) {
-  const size_t col_smem = sizeof(float2) * 2 * CW * p.Fr;
-  int rc = set_smem(fft_cols<MODE, CW>, col_smem);
+  const int T = p.Fr / 16, cw = kColThreads / T;
+  const size_t smem = sizeof(float2) * (size_t)cw * (p.Fr + p.Fr / 16);
+  int rc = set_smem(fft_cols<MODE>, smem);
   if (rc) return rc;
-  const int cblocks = (p.Fc / 2 + 1 + CW - 1) / CW;
-  fft_cols<MODE, CW><<<cblocks * planes, kFftThreads, col_smem, st>>>(p, spec, G, planes);
+  const int cblocks = (p.Fc / 2 + 1 + cw - 1) / cw;
+  fft_cols<MODE><<<cblocks * planes, kColThreads, smem, st>>>(p, spec, G, planes);
   return CCT_OK;
 }
 
+// Rows per CTA and shared memory of the row passes.
+void row_shape(const FftParams &p, int rows, int *per, int *blocks, size_t *smem) {
+  const int N = p.Fc / 2, T = N / 16;
+  *per = kRowThreads / T;
+  *blocks = (rows + *per - 1) / *per;
+  *smem = sizeof(float2) * (size_t)(*per) * (N + N / 16);
+}
+
 int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cudaStream_t st) {
-  const size_t row_smem = sizeof(float2) * p.Fc;  // a + b of Fc/2 each
-  int rc = set_smem(fft_rows_r2c<1>, row_smem);
-  if (rc) return rc;
   const int planes = p.g.pf;
-  fft_rows_r2c<1><<<p.Fr * planes, kFftThreads, row_smem, st>>>(p, f, G, planes);
-  rc = col_width(p.Fr) == 4 ? launch_cols<1, 4>(p, G, nullptr, planes, st)
-                            : launch_cols<1, 2>(p, G, nullptr, planes, st);
+  int per, blocks;
+  size_t smem;
+  row_shape(p, p.Fr * planes, &per, &blocks, &smem);
+  int rc = set_smem(fft_rows_r2c<1>, smem);
+  if (rc) return rc;
+  fft_rows_r2c<1><<<blocks, per * (p.Fc / 32), smem, st>>>(p, f, G, planes);
+  rc = launch_cols<1>(p, G, nullptr, planes, st);
   if (rc) return rc;
   count_launches(2);
   return check_cuda(cudaGetLastError(), "fft filter spectrum launch");
@@ -416,16 +558,18 @@ int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cu
 
 int launch_fft_conv(const FftParams &p, const float *x, const float2 *G, float2 *spec, float *y,
                     cudaStream_t st) {
-  const size_t row_smem = sizeof(float2) * p.Fc;
-  int rc = set_smem(fft_rows_r2c<0>, row_smem);
-  if (!rc) rc = set_smem(fft_rows_c2r, row_smem);
-  if (rc) return rc;
   const int planes = p.g.pout;
-  fft_rows_r2c<0><<<p.Fr * planes, kFftThreads, row_smem, st>>>(p, x, spec, planes);
-  rc = col_width(p.Fr) == 4 ? launch_cols<0, 4>(p, spec, G, planes, st)
-                            : launch_cols<0, 2>(p, spec, G, planes, st);
+  int per, blocks, cper, cblocks;
+  size_t smem, csmem;
+  row_shape(p, p.Fr * planes, &per, &blocks, &smem);
+  row_shape(p, p.g.OH * planes, &cper, &cblocks, &csmem);
+  int rc = set_smem(fft_rows_r2c<0>, smem);
+  if (!rc) rc = set_smem(fft_rows_c2r, csmem);
   if (rc) return rc;
-  fft_rows_c2r<<<p.g.OH * planes, kFftThreads, row_smem, st>>>(p, spec, y, planes);
+  fft_rows_r2c<0><<<blocks, per * (p.Fc / 32), smem, st>>>(p, x, spec, planes);
+  rc = launch_cols<0>(p, spec, G, planes, st);
+  if (rc) return rc;
+  fft_rows_c2r<<<cblocks, cper * (p.Fc / 32), csmem, st>>>(p, spec, y, planes);
   count_launches(3);
   return check_cuda(cudaGetLastError(), "fft convolution launch");
 }

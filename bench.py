@@ -77,12 +77,20 @@ def barrier(pg):
 
 
 def max_over_ranks(pg, value):
+    """The slowest rank's time: every rank takes the same all-reduce."""
     import torch
     if pg is None:
         return value
-    t = torch.tensor([value], device="cuda", dtype=torch.float64)
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], device=dev, dtype=torch.float64)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(units_per_rank, world, t_max):
+    """Whole-job rate of N identical replicas: all ranks' units over the
+    slowest rank's time."""
+    return world * units_per_rank / t_max
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -750,13 +758,13 @@ def main():
 
     if wl.get("fft_hbm_roofline"):
         # FFT: reported in direct-equivalent GFLOP/s; its roofline is HBM
-        value = world * wl["gflop_per_step"] * args.steps / t_max
-        e2e_val = world * wl["gflop_per_step"] * e2e_steps / e2e_t
+        value = replica_value(wl["gflop_per_step"] * args.steps, world, t_max)
+        e2e_val = replica_value(wl["gflop_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["bytes_per_launch"] / per_launch / 1e9
         bound, peak, unit = "hbm", peaks["hbm_gbs"], "GB/s"
     elif wl["unit"] == "GFLOP/s":
-        value = world * wl["gflop_per_step"] * args.steps / t_max
-        e2e_val = world * wl["gflop_per_step"] * e2e_steps / e2e_t
+        value = replica_value(wl["gflop_per_step"] * args.steps, world, t_max)
+        e2e_val = replica_value(wl["gflop_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["gflop_per_launch"] / per_launch / 1e3  # TFLOP/s
         if wl["precision"] == "bf16x3":
             bound, peak, unit = "tensor", peaks["bf16_tflops"], "TFLOP/s"
@@ -765,8 +773,8 @@ def main():
             bound, unit = "fp32_simt", "TFLOP/s"
             peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) / 1e6
     else:
-        value = world * wl["bytes_per_step"] * args.steps / t_max / 1e9
-        e2e_val = world * wl["e2e_gb_per_step"] * e2e_steps / e2e_t
+        value = replica_value(wl["bytes_per_step"] * args.steps, world, t_max) / 1e9
+        e2e_val = replica_value(wl["e2e_gb_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["bytes_per_launch"] / per_launch / 1e9
         bound, peak, unit = "hbm", peaks["hbm_gbs"], "GB/s"
 

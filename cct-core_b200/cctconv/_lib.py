@@ -22,7 +22,7 @@ SAMPLE_NONE, SAMPLE_DOWN, SAMPLE_UP = 0, 1, 2
 PREC_FP32, PREC_BF16X3 = 0, 1
 ALGO_AUTO, ALGO_DIRECT, ALGO_FFT = 0, 1, 2
 FLAG_RELU = 0x1
-PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT = 0, 1, 2, 3
+PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT, PLAN_FILTER_ADJOINT = 0, 1, 2, 3, 4
 
 
 class ConvDesc(ctypes.Structure):
@@ -115,6 +115,7 @@ SIGNATURES = {
     "cct_stream_destroy": (_I, [_P]),
     "cct_stream_synchronize": (_I, [_P]),
     "cct_device_status": (_I, []),
+    "cct_selftest_wait_timeout": (_I, [ctypes.POINTER(ctypes.c_double)]),
     "cct_last_error_string": (ctypes.c_char_p, []),
     "cct_abi_version": (_I, []),
     "cct_launch_count": (ctypes.c_uint64, []),

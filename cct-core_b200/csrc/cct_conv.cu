@@ -199,7 +199,7 @@ int resolve_geom(const cct_conv_desc *desc, ConvGeom *g) { return resolve(desc, 
 
 using namespace cct;
 
-enum { ALGO_DIRECT = 0, ALGO_FRAME_F32 = 1, ALGO_FRAME_BF16X3 = 2, ALGO_FFT = 3 };
+enum { ALGO_DIRECT = 0, ALGO_FRAME_F32 = 1, ALGO_FRAME_BF16X3 = 2, ALGO_FFT = 3, ALGO_FILTER_ADJOINT = 4 };
 
 struct cct_conv_plan {
   cct_conv_desc desc;
@@ -217,6 +217,7 @@ struct cct_conv_plan {
   float2 *fft_filter;    // filter spectrum
   float2 *fft_tw;        // twiddle tables
   bool fft_static;       // fft_filter holds the static filter's FP64 spectrum
+  float *fa_work;        // per-image FilterAdjoint results before the block reduce
   // run_host staging (allocated on the first cct_conv_run_host call)
   float *d_x, *d_f, *d_y;
 };
@@ -299,6 +300,8 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
     return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
   if (use_fft)
     algo = ALGO_FFT;
+  else if (fa_f32_supported(g))
+    algo = ALGO_FILTER_ADJOINT;
   else if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
     algo = ALGO_FRAME_BF16X3;
   else
@@ -322,6 +325,13 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
     rc = check_cuda(cudaMalloc(&p->packed, tc.pack_bytes), "cudaMalloc(packed filters)");
     if (rc) {
       delete p;
+      return rc;
+    }
+  }
+  if (algo == ALGO_FILTER_ADJOINT && fa_workspace_bytes(g)) {
+    rc = check_cuda(cudaMalloc(&p->fa_work, fa_workspace_bytes(g)), "cudaMalloc(FilterAdjoint workspace)");
+    if (rc) {
+      cct_conv_plan_destroy(p);
       return rc;
     }
   }
@@ -355,6 +365,7 @@ int cct_conv_plan_destroy(cct_conv_plan *p) {
   cudaFree(p->fft_spec);
   cudaFree(p->fft_filter);
   cudaFree(p->fft_tw);
+  cudaFree(p->fa_work);
   cudaFree(p->d_x);
   cudaFree(p->d_f);
   cudaFree(p->d_y);
@@ -413,6 +424,8 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
     }
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);
+    case ALGO_FILTER_ADJOINT:
+      return launch_fa_f32(p->g, x, f, y, p->fa_work, st);
     case ALGO_FFT: {
       int rc = CCT_OK;
       if (f != p->static_filter || !p->fft_static)

@@ -99,6 +99,12 @@ int launch_direct_tma(const ConvGeom &g, const float *x, const float *f, float *
 // Per-device error word passed to kernels with bounded waits (allocated on
 // first use on the current device).
 unsigned *device_error_word();
+// FilterAdjoint with small results (fa_f32.cu): BorderValid, no sampling,
+// result width <= 8.  The block-reduced form needs fa_workspace_bytes() of
+// plan workspace.
+bool fa_f32_supported(const ConvGeom &g);
+size_t fa_workspace_bytes(const ConvGeom &g);
+int launch_fa_f32(const ConvGeom &g, const float *x, const float *f, float *y, float *work, cudaStream_t st);
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);

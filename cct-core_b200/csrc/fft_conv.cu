@@ -38,6 +38,7 @@ namespace {
 
 constexpr int kRowThreads = 256;
 constexpr int kColThreads = 512;
+__host__ __device__ constexpr int col_stride(int Fr) { return Fr + Fr / 16 + 8; }
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -168,46 +169,21 @@ __device__ __forceinline__ void pass_store(float2 *s, const float2 (&v)[16], int
   }
 }
 
-// N-point FFT (N = 2^logN >= 16) of the sequence whose first-pass inputs
+// N-point FFT (N = 2^LOGN >= 16) of the sequence whose first-pass inputs
 // v[m] = x[tt + m*T] the caller loaded; the result lands in natural order in
-// s (padded).  Every thread of the CTA calls this with the same N.
-template <bool INV>
-__device__ void fft_seq(float2 *s, float2 (&v)[16], int N, int logN, int T, int tt,
-                        const float2 *__restrict__ tw) {
-  int Ns = 1, rem = logN;
-  bool first = true;
-  while (rem > 0) {
-    const int b = rem >= 4 ? 4 : rem;
-    switch (b) {
-      case 4:
-        if (!first) pass_load<16>(s, v, N, T, tt);
-        pass_compute<16, INV>(v, N, Ns, T, tt, tw);
-        __syncthreads();
-        pass_store<16>(s, v, Ns, T, tt);
-        break;
-      case 3:
-        if (!first) pass_load<8>(s, v, N, T, tt);
-        pass_compute<8, INV>(v, N, Ns, T, tt, tw);
-        __syncthreads();
-        pass_store<8>(s, v, Ns, T, tt);
-        break;
-      case 2:
-        if (!first) pass_load<4>(s, v, N, T, tt);
-        pass_compute<4, INV>(v, N, Ns, T, tt, tw);
-        __syncthreads();
-        pass_store<4>(s, v, Ns, T, tt);
-        break;
-      default:
-        if (!first) pass_load<2>(s, v, N, T, tt);
-        pass_compute<2, INV>(v, N, Ns, T, tt, tw);
-        __syncthreads();
-        pass_store<2>(s, v, Ns, T, tt);
-        break;
-    }
+// s (padded).  The passes (radix 16, the last 2..16) are fixed at compile
+// time.  Every thread of the CTA takes part (the passes synchronise the CTA).
+template <int LOGN, bool INV, int NS_LOG = 0, bool FIRST = true>
+__device__ __forceinline__ void fft_passes(float2 *s, float2 (&v)[16], int tt, const float2 *__restrict__ tw) {
+  if constexpr (NS_LOG < LOGN) {
+    constexpr int B = (LOGN - NS_LOG) >= 4 ? 4 : (LOGN - NS_LOG);
+    constexpr int R = 1 << B, N = 1 << LOGN, T = N / 16;
+    if (!FIRST) pass_load<R>(s, v, N, T, tt);
+    pass_compute<R, INV>(v, N, 1 << NS_LOG, T, tt, tw);
     __syncthreads();
-    Ns <<= b;
-    rem -= b;
-    first = false;
+    pass_store<R>(s, v, 1 << NS_LOG, T, tt);
+    __syncthreads();
+    fft_passes<LOGN, INV, NS_LOG + B, false>(s, v, tt, tw);
   }
 }
 
@@ -235,11 +211,11 @@ __device__ __forceinline__ int filter_index(int pos, int h, int R, int F, bool c
 // Row pass: rows_per_cta sequences of N = Fc/2 complex points per CTA.
 // SRC 0: image plane rows expanded with the border; 1: filter plane rows
 // centred at the origin (flipped for convolution).
-template <int SRC>
-__global__ void __launch_bounds__(kRowThreads)
+template <int SRC, int LOGN>
+__global__ void __launch_bounds__(kRowThreads, 4)
     fft_rows_r2c(FftParams p, const float *__restrict__ src, float2 *__restrict__ spec, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int N = p.Fc / 2, T = N / 16, per = blockDim.x / T;
+  constexpr int N = 1 << LOGN, T = N / 16, per = kRowThreads / T;
   const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
   const int gr = blockIdx.x * per + sub;
   const bool active = gr < planes * p.Fr;
@@ -281,7 +257,7 @@ __global__ void __launch_bounds__(kRowThreads)
       v[m] = make_float2(e[0], e[1]);
     }
   }
-  fft_seq<false>(s, v, N, p.logN, T, tt, p.tw_n);
+  fft_passes<LOGN, false>(s, v, tt, p.tw_n);
   if (!active) return;
   // X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i,
   // W = exp(-2 pi i / Fc), k = 0..N
@@ -299,21 +275,24 @@ __global__ void __launch_bounds__(kRowThreads)
 // threads, so each warp reads 32-byte row segments).
 // MODE 0: forward FFT, times G[fplane], inverse FFT, in place in spec.
 // MODE 1: forward FFT and scaling by p.scale (a filter's spectrum).
-template <int MODE>
-__global__ void __launch_bounds__(kColThreads)
+template <int MODE, int LOGR>
+__global__ void __launch_bounds__(kColThreads, 2)
     fft_cols(FftParams p, float2 *__restrict__ spec, const float2 *__restrict__ G, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
-  const int Fr = p.Fr, T = Fr / 16, CW = blockDim.x / T, ncol = p.Fc / 2 + 1;
+  constexpr int Fr = 1 << LOGR, T = Fr / 16, CW = kColThreads / T;
+  const int ncol = p.Fc / 2 + 1;
   const int cblocks = (ncol + CW - 1) / CW;
   const int pl = blockIdx.x / cblocks, c0 = (blockIdx.x - pl * cblocks) * CW;
   const int c = threadIdx.x % CW, tt = threadIdx.x / CW, col = c0 + c;
   const bool active = col < ncol;
-  float2 *s = fsm + c * (Fr + Fr / 16);
+  // column stride = 8 (mod 16) complex: the CW columns a warp touches fall
+  // on alternate halves of the banks
+  float2 *s = fsm + c * col_stride(Fr);
   float2 *sp = spec + (size_t)pl * Fr * p.ld + col;
   float2 v[16];
 #pragma unroll
   for (int m = 0; m < 16; ++m) v[m] = active ? sp[(size_t)(tt + m * T) * p.ld] : make_float2(0.0f, 0.0f);
-  fft_seq<false>(s, v, Fr, p.logR, T, tt, p.tw_r);
+  fft_passes<LOGR, false>(s, v, tt, p.tw_r);
   if (MODE == 0) {
     int ip, fp;
     plane_pair(p.g, pl, 0, &ip, &fp);
@@ -323,7 +302,7 @@ __global__ void __launch_bounds__(kColThreads)
       const int r = tt + m * T;
       v[m] = active ? cmul(s[pad16(r)], __ldg(gp + (size_t)r * p.ld)) : make_float2(0.0f, 0.0f);
     }
-    fft_seq<true>(s, v, Fr, p.logR, T, tt, p.tw_r);
+    fft_passes<LOGR, true>(s, v, tt, p.tw_r);
     if (!active) return;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
@@ -341,11 +320,12 @@ __global__ void __launch_bounds__(kColThreads)
 }
 
 // Inverse row pass: half-spectrum rows -> real rows, trimmed to the output.
-__global__ void __launch_bounds__(kRowThreads)
+template <int LOGN>
+__global__ void __launch_bounds__(kRowThreads, 4)
     fft_rows_c2r(FftParams p, const float2 *__restrict__ spec, float *__restrict__ y, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
   const ConvGeom &g = p.g;
-  const int N = p.Fc / 2, T = N / 16, per = blockDim.x / T;
+  constexpr int N = 1 << LOGN, T = N / 16, per = kRowThreads / T;
   const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
   const int gr = blockIdx.x * per + sub;
   const bool active = gr < planes * g.OH;
@@ -367,7 +347,7 @@ __global__ void __launch_bounds__(kRowThreads)
     }
     v[m] = z;
   }
-  fft_seq<true>(s, v, N, p.logN, T, tt, p.tw_n);
+  fft_passes<LOGN, true>(s, v, tt, p.tw_n);
   if (!active) return;
   float *yr = y + ((size_t)pl * g.OH + row) * g.OW;
   const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
@@ -523,14 +503,35 @@ void fft_static_spectrum(const FftParams &p, const float *host_filter, std::vect
   }
 }
 
-template <int MODE>
-int launch_cols(const FftParams &p, float2 *spec, const float2 *G, int planes, cudaStream_t st) {
-  const int T = p.Fr / 16, cw = kColThreads / T;
-  const size_t smem = sizeof(float2) * (size_t)cw * (p.Fr + p.Fr / 16);
-  int rc = set_smem(fft_cols<MODE>, smem);
+// Kernel instantiation for the transform length (2^4 .. 2^12 points).
+#define CCT_FFT_LOG_SWITCH(LOGV, CALL)                     \
+  switch (LOGV) {                                          \
+    case 4: { constexpr int L = 4; CALL; } break;          \
+    case 5: { constexpr int L = 5; CALL; } break;          \
+    case 6: { constexpr int L = 6; CALL; } break;          \
+    case 7: { constexpr int L = 7; CALL; } break;          \
+    case 8: { constexpr int L = 8; CALL; } break;          \
+    case 9: { constexpr int L = 9; CALL; } break;          \
+    case 10: { constexpr int L = 10; CALL; } break;        \
+    case 11: { constexpr int L = 11; CALL; } break;        \
+    case 12: { constexpr int L = 12; CALL; } break;        \
+    default: return set_error(CCT_ENOTSUP, "FFT length 2^%d", (int)(LOGV)); \
+  }
+
+template <int MODE, int L>
+int launch_cols_t(const FftParams &p, float2 *spec, const float2 *G, int planes, cudaStream_t st) {
+  constexpr int Fr = 1 << L, cw = kColThreads / (Fr / 16);
+  const size_t smem = sizeof(float2) * (size_t)cw * col_stride(Fr);
+  int rc = set_smem(fft_cols<MODE, L>, smem);
   if (rc) return rc;
   const int cblocks = (p.Fc / 2 + 1 + cw - 1) / cw;
-  fft_cols<MODE><<<cblocks * planes, kColThreads, smem, st>>>(p, spec, G, planes);
+  fft_cols<MODE, L><<<cblocks * planes, kColThreads, smem, st>>>(p, spec, G, planes);
+  return CCT_OK;
+}
+
+template <int MODE>
+int launch_cols(const FftParams &p, float2 *spec, const float2 *G, int planes, cudaStream_t st) {
+  CCT_FFT_LOG_SWITCH(p.logR, return (launch_cols_t<MODE, L>(p, spec, G, planes, st)))
   return CCT_OK;
 }
 
@@ -542,15 +543,33 @@ void row_shape(const FftParams &p, int rows, int *per, int *blocks, size_t *smem
   *smem = sizeof(float2) * (size_t)(*per) * (N + N / 16);
 }
 
-int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cudaStream_t st) {
-  const int planes = p.g.pf;
+template <int SRC, int L>
+int launch_r2c_t(const FftParams &p, const float *src, float2 *spec, int planes, cudaStream_t st) {
   int per, blocks;
   size_t smem;
   row_shape(p, p.Fr * planes, &per, &blocks, &smem);
-  int rc = set_smem(fft_rows_r2c<1>, smem);
+  int rc = set_smem(fft_rows_r2c<SRC, L>, smem);
   if (rc) return rc;
-  fft_rows_r2c<1><<<blocks, per * (p.Fc / 32), smem, st>>>(p, f, G, planes);
-  rc = launch_cols<1>(p, G, nullptr, planes, st);
+  fft_rows_r2c<SRC, L><<<blocks, kRowThreads, smem, st>>>(p, src, spec, planes);
+  return CCT_OK;
+}
+
+template <int L>
+int launch_c2r_t(const FftParams &p, const float2 *spec, float *y, int planes, cudaStream_t st) {
+  int per, blocks;
+  size_t smem;
+  row_shape(p, p.g.OH * planes, &per, &blocks, &smem);
+  int rc = set_smem(fft_rows_c2r<L>, smem);
+  if (rc) return rc;
+  fft_rows_c2r<L><<<blocks, kRowThreads, smem, st>>>(p, spec, y, planes);
+  return CCT_OK;
+}
+
+int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cudaStream_t st) {
+  const int planes = p.g.pf;
+  int rc = CCT_OK;
+  CCT_FFT_LOG_SWITCH(p.logN, rc = (launch_r2c_t<1, L>(p, f, G, planes, st)))
+  if (!rc) rc = launch_cols<1>(p, G, nullptr, planes, st);
   if (rc) return rc;
   count_launches(2);
   return check_cuda(cudaGetLastError(), "fft filter spectrum launch");
@@ -559,17 +578,12 @@ int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cu
 int launch_fft_conv(const FftParams &p, const float *x, const float2 *G, float2 *spec, float *y,
                     cudaStream_t st) {
   const int planes = p.g.pout;
-  int per, blocks, cper, cblocks;
-  size_t smem, csmem;
-  row_shape(p, p.Fr * planes, &per, &blocks, &smem);
-  row_shape(p, p.g.OH * planes, &cper, &cblocks, &csmem);
-  int rc = set_smem(fft_rows_r2c<0>, smem);
-  if (!rc) rc = set_smem(fft_rows_c2r, csmem);
+  int rc = CCT_OK;
+  CCT_FFT_LOG_SWITCH(p.logN, rc = (launch_r2c_t<0, L>(p, x, spec, planes, st)))
+  if (!rc) rc = launch_cols<0>(p, spec, G, planes, st);
   if (rc) return rc;
-  fft_rows_r2c<0><<<blocks, per * (p.Fc / 32), smem, st>>>(p, x, spec, planes);
-  rc = launch_cols<0>(p, spec, G, planes, st);
+  CCT_FFT_LOG_SWITCH(p.logN, rc = (launch_c2r_t<L>(p, spec, y, planes, st)))
   if (rc) return rc;
-  fft_rows_c2r<<<cblocks, cper * (p.Fc / 32), csmem, st>>>(p, spec, y, planes);
   count_launches(3);
   return check_cuda(cudaGetLastError(), "fft convolution launch");
 }

@@ -13,10 +13,19 @@ namespace cct {
 // cct_device_status().
 constexpr unsigned kErrWaitTimeout = 1u;
 
-// Upper bound on mbarrier polls before a wait gives up.  Each try_wait
-// suspends for up to the hardware's time limit, so this is seconds of
-// waiting -- only reachable if a copy never lands.
-constexpr uint32_t kMaxWaitPolls = 1u << 22;
+// A bounded wait gives up after this much device time (about one second),
+// sets kErrWaitTimeout and lets the kernel return: the context stays usable
+// and the host reads the status.  Only reachable if a copy or an arrival
+// never comes.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
+// Secondary bound on polls, in case the global timer does not advance.
+constexpr uint32_t kMaxWaitPolls = 1u << 26;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -56,6 +65,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsign
   // only when the phase is still open.
   if (mbar_test(bar, parity)) return true;
   const uint32_t addr = smem_u32(bar);
+  const uint64_t t0 = global_ns();
   for (uint32_t i = 0; i < kMaxWaitPolls; ++i) {
     uint32_t done;
     asm volatile(
@@ -65,6 +75,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsign
         : "r"(addr), "r"(parity)
         : "memory");
     if (done) return true;
+    if ((i & 63) == 63 && global_ns() - t0 > kWaitLimitNs) break;
   }
   atomicOr(err, kErrWaitTimeout);
   return false;

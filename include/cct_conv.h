@@ -116,7 +116,7 @@ int cct_conv_plan_create(const cct_conv_desc *desc, cct_conv_plan **plan);
 int cct_conv_plan_destroy(cct_conv_plan *plan);
 
 /* Kernel family the plan chose: 0 direct stencil, 1 frame FP32, 2 frame
- * BF16X3 tensor core, 3 FFT. */
+ * BF16X3 tensor core, 3 FFT, 4 FilterAdjoint FP32. */
 int cct_conv_plan_algo(const cct_conv_plan *plan, int32_t *algo_out);
 
 /* Static filter (the reference's ConstantFieldKernel filter): its FFT
@@ -294,6 +294,13 @@ int cct_stream_synchronize(void *stream);
  * (src/main/scala/cogx/platform/opencl/OpenCLDeviceKernel.scala:106-147).
  * Reading clears the status; the call synchronises with the device. */
 int cct_device_status(void);
+/* Failure-detection self-test (no counterpart in the reference): launches a
+ * kernel whose mbarrier wait never completes, so the library's bounded wait
+ * gives up after about one second, records the timeout and returns.  Returns
+ * CCT_OK when the kernel came back on its own (elapsed_ms, may be NULL, is the
+ * host-side duration); the following cct_device_status() then reports
+ * CCT_ETIMEOUT, and the context stays usable. */
+int cct_selftest_wait_timeout(double *elapsed_ms);
 const char *cct_last_error_string(void);
 int cct_abi_version(void);
 /* Kernel launches issued by this process so far (all plans, all threads). */

@@ -79,3 +79,53 @@ def test_filter_adjoint_api_and_scalar_result():
     assert torch.equal(acc, red)
     with pytest.raises(ValueError, match="multiple of the batchSize"):
         C.crossCorrelateFilterAdjoint(xv, gv[:7], C.BorderValid, batchSize=2)
+
+
+def test_small_results_take_the_filter_adjoint_kernel():
+    """BorderValid, unsampled, results up to 8 wide run on the dedicated
+    FilterAdjoint kernel; up-sampled gradients stay on the generic kernel."""
+    def algo(sampling, step, out):
+        d = _lib.new_desc(image_rows=64 + out - 1, image_cols=64 + out - 1, image_planes=2 * 32,
+                          filter_rows=64, filter_cols=64, filter_planes=2 * 64, batch_size=2,
+                          border=_lib.BORDER_VALID, orientation=_lib.CROSS_CORRELATION,
+                          sampling=sampling, step=step, vector_mode=_lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM)
+        p = _lib.Plan(d)
+        a = p.algo
+        p.close()
+        return a
+    assert algo(_lib.SAMPLE_NONE, 1, 5) == _lib.PLAN_FILTER_ADJOINT
+    assert algo(_lib.SAMPLE_NONE, 1, 9) == _lib.PLAN_DIRECT
+
+
+def test_filter_adjoint_weight_gradient_timing():
+    """The weight gradient of the B=16, C=32, K=64, 64x64, 5x5 layer: image
+    padded to 68x68, gradient 64x64, 2048 result planes of 5x5."""
+    B, Cn, K = 16, 32, 64
+    rng = np.random.default_rng(7)
+    x = torch.from_numpy(rng.standard_normal((B * Cn, 68, 68)).astype(np.float32)).cuda()
+    g = torch.from_numpy(rng.standard_normal((B * K, 64, 64)).astype(np.float32)).cuda()
+    d = _lib.new_desc(image_rows=68, image_cols=68, image_planes=B * Cn, filter_rows=64, filter_cols=64,
+                      filter_planes=B * K, batch_size=B, border=_lib.BORDER_VALID,
+                      orientation=_lib.CROSS_CORRELATION, vector_mode=_lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM)
+    plan = _lib.Plan(d)
+    assert plan.algo == _lib.PLAN_FILTER_ADJOINT
+    y = torch.empty((Cn * K, 5, 5), device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        plan.run(x.data_ptr(), g.data_ptr(), y.data_ptr(), st)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(10):
+        plan.run(x.data_ptr(), g.data_ptr(), y.data_ptr(), st)
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b) / 10
+    print(f"weight gradient B=16 C=32 K=64 64x64 5x5: {ms:.3f} ms, "
+          f"{2 * B * Cn * K * 64 * 64 * 25 / ms / 1e9:.1f} GFLOP/s")
+    # spot-check planes against the oracle
+    od = O.make_desc(68, 68, 64, 64, planes=B * Cn, f_planes=B * K, batch=B, border=O.VALID,
+                     orient=O.XCORR, mode=O.FILTER_ADJOINT_REDUCE)
+    ref = O.conv(od, x.cpu().numpy(), g.cpu().numpy(), np.float32).reshape(Cn * K, 5, 5)
+    got = y.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    plan.close()

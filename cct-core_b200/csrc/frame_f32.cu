@@ -84,11 +84,15 @@ __global__ void __launch_bounds__(kThreads, 2)
     cp_async_commit();
   };
 
-  float acc[kU][kKT];
+  // Output planes k, k+1 advance together in packed fma.rn.f32x2 / add.rn.f32x2
+  // (each lane the same RN operation as the scalar form, so the order and
+  // the result per output are unchanged).
+  constexpr int kP = kKT / 2;
+  float2 acc[kU][kP];
 #pragma unroll
   for (int u = 0; u < kU; ++u)
 #pragma unroll
-    for (int k = 0; k < kKT; ++k) acc[u][k] = 0.0f;
+    for (int k = 0; k < kP; ++k) acc[u][k] = make_float2(0.0f, 0.0f);
 
   issue(0, 0);
   for (int t = 0; t < g.terms; ++t) {
@@ -103,11 +107,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     const float *ft = tile + T::TILE + grp * kKT;
     const float *base = tile + (ty * DOWN) * T::PITCH + tx * kU * DOWN;
 
-    float rs[kU][kKT];
+    float2 rs[kU][kP];
 #pragma unroll
     for (int u = 0; u < kU; ++u)
 #pragma unroll
-      for (int k = 0; k < kKT; ++k) rs[u][k] = 0.0f;
+      for (int k = 0; k < kP; ++k) rs[u][k] = make_float2(0.0f, 0.0f);
 
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -120,33 +124,34 @@ __global__ void __launch_bounds__(kThreads, 2)
         vals[4 * e + 2] = q.z;
         vals[4 * e + 3] = q.w;
       }
-      float cs[kU][kKT];
+      float2 cs[kU][kP];
 #pragma unroll
       for (int s = 0; s < S; ++s) {
-        float w[kKT];
+        float2 w[kP];
 #pragma unroll
         for (int k4 = 0; k4 < kKT / 4; ++k4) {
           const float4 q = *reinterpret_cast<const float4 *>(ft + (r * S + s) * kKB + 4 * k4);
-          w[4 * k4 + 0] = q.x;
-          w[4 * k4 + 1] = q.y;
-          w[4 * k4 + 2] = q.z;
-          w[4 * k4 + 3] = q.w;
+          w[2 * k4 + 0] = make_float2(q.x, q.y);
+          w[2 * k4 + 1] = make_float2(q.z, q.w);
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u)
+        for (int u = 0; u < kU; ++u) {
+          const float xv = vals[u * DOWN + s];
+          const float2 x2 = make_float2(xv, xv);
 #pragma unroll
-          for (int k = 0; k < kKT; ++k)
-            cs[u][k] = __fmaf_rn(vals[u * DOWN + s], w[k], s == 0 ? 0.0f : cs[u][k]);
+          for (int k = 0; k < kP; ++k)
+            cs[u][k] = __ffma2_rn(x2, w[k], s == 0 ? make_float2(0.0f, 0.0f) : cs[u][k]);
+        }
       }
 #pragma unroll
       for (int u = 0; u < kU; ++u)
 #pragma unroll
-        for (int k = 0; k < kKT; ++k) rs[u][k] = __fadd_rn(rs[u][k], cs[u][k]);
+        for (int k = 0; k < kP; ++k) rs[u][k] = __fadd2_rn(rs[u][k], cs[u][k]);
     }
 #pragma unroll
     for (int u = 0; u < kU; ++u)
 #pragma unroll
-      for (int k = 0; k < kKT; ++k) acc[u][k] = (t == 0) ? rs[u][k] : __fadd_rn(acc[u][k], rs[u][k]);
+      for (int k = 0; k < kP; ++k) acc[u][k] = (t == 0) ? rs[u][k] : __fadd2_rn(acc[u][k], rs[u][k]);
     __syncthreads();
   }
 
@@ -162,7 +167,8 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
     for (int u = 0; u < kU; ++u) {
       const int col = out_c0 + tx * kU + u;
-      if (col < g.OW) ys[col] = relu ? fmaxf(acc[u][k], 0.0f) : acc[u][k];
+      const float a = (k & 1) ? acc[u][k >> 1].y : acc[u][k >> 1].x;
+      if (col < g.OW) ys[col] = relu ? fmaxf(a, 0.0f) : a;
     }
   }
 }

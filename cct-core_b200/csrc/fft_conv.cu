@@ -140,10 +140,26 @@ __device__ __forceinline__ void pass_compute(float2 (&v)[16], int N, int Ns, int
   for (int q = 0; q < 16 / R; ++q) {
     const int j = tt + q * T, k = j & (Ns - 1);
     if (k) {
+      // w^m for m < R from two table reads (w and w^4) and at most two
+      // products (w^m = (w^4)^a w^b, m = 4a + b), instead of R-1 scattered
+      // reads per butterfly
       const int step = N / (Ns * R);
+      float2 p[4], p4[4];
+      p[0] = make_float2(1.0f, 0.0f);
+      p[1] = __ldg(tw + k * step);
+      if (R > 2) {
+        p[2] = cmul(p[1], p[1]);
+        p[3] = cmul(p[2], p[1]);
+      }
+      if (R > 4) {
+        p4[0] = make_float2(1.0f, 0.0f);
+        p4[1] = __ldg(tw + 4 * k * step);
+        p4[2] = cmul(p4[1], p4[1]);
+        p4[3] = cmul(p4[2], p4[1]);
+      }
 #pragma unroll
       for (int m = 1; m < R; ++m) {
-        const float2 w = __ldg(tw + m * k * step);
+        const float2 w = (m < 4) ? p[m] : ((m & 3) ? cmul(p4[m >> 2], p[m & 3]) : p4[m >> 2]);
         v[q * R + m] = cmul(v[q * R + m], INV ? conjf2(w) : w);
       }
     }

@@ -372,18 +372,19 @@ __global__ void __launch_bounds__(kThreads, 1)
 // with tap' flipped for convolution.  Rows/columns past the real counts are 0.
 __global__ void pack_filters_kernel(ConvGeom g, const float *__restrict__ f, uint8_t *__restrict__ out,
                                     int NT, int CB, int NCB, int nblocks) {
+  // the packed operand is at most a few hundred MB, so 32-bit indices suffice
+  // (launch_pack_filters checks); 64-bit division would dominate this kernel
   const int RS = g.R * g.S;
-  const long long total = (long long)nblocks * NCB * RS * NT * CB;
-  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
-       idx += (long long)gridDim.x * blockDim.x) {
-    const int ci = (int)(idx % CB);
-    long long rest = idx / CB;
-    const int n = (int)(rest % NT);
+  const int total = nblocks * NCB * RS * NT * CB;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int ci = idx % CB;
+    int rest = idx / CB;
+    const int n = rest % NT;
     rest /= NT;
-    const int tap = (int)(rest % RS);
+    const int tap = rest % RS;
     rest /= RS;
-    const int cb = (int)(rest % NCB);
-    const int nb = (int)(rest / NCB);
+    const int cb = rest % NCB;
+    const int nb = rest / NCB;
     const int k = nb * NT + n, c = cb * CB + ci;
     float v = 0.0f;
     if (k < g.groups && c < g.n) {
@@ -492,6 +493,7 @@ bool frame_tc_plan(const ConvGeom &g, int sms, TcParams *out) {
 
 int launch_pack_filters(const TcParams &p, const float *f, uint8_t *packed, cudaStream_t st) {
   const long long total = (long long)p.nblocks * p.NCB * p.g.R * p.g.S * p.NT * p.CB;
+  if (total > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "packed filter operand too large");
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
   pack_filters_kernel<<<blocks, 256, 0, st>>>(p.g, f, packed, p.NT, p.CB, p.NCB, p.nblocks);
   count_launches(1);

@@ -25,6 +25,7 @@
 #include <memory>
 #include <mutex>
 #include <set>
+#include <string>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -224,6 +225,7 @@ struct Req {
   Clock::time_point t_submit;
   double latency_us = 0.0;
   int status = CCT_OK;
+  std::string msg;  // the scheduler thread's error text, for the waiting thread
   bool done = false;
   double flops = 0.0;
 };
@@ -362,6 +364,7 @@ void fill_item(cct_server *s, const Req &q, Item *it) {
 
 void finish(cct_server *s, Req &q, int status, Clock::time_point t) {
   q.status = status;
+  if (status != CCT_OK) q.msg = cct_last_error_string();
   q.latency_us = std::chrono::duration<double, std::micro>(t - q.t_submit).count();
   if (q.r.kind == CCT_SERVE_CONV) s->arena.release(q.off, q.bytes);
   q.done = true;
@@ -800,7 +803,8 @@ int cct_server_wait(cct_server *s, uint64_t ticket, int32_t timeout_ms, double *
   }
   if (latency_us) *latency_us = q->latency_us;
   s->table.erase(ticket);
-  return q->status;
+  if (q->status != CCT_OK) return set_error(q->status, "request %llu: %s", (unsigned long long)ticket, q->msg.c_str());
+  return CCT_OK;
 }
 
 int cct_server_replay(cct_server *s, const cct_serve_request *reqs, const double *arrival_s, int32_t n,

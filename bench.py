@@ -269,16 +269,38 @@ def plain_workload():
     def e2e_step():
         plan64.run_host(hx.data_ptr(), hf.data_ptr(), hy.data_ptr(), stream)
 
+    # beside it: the single 256x256 plane (L2-resident, launch-bound) and the
+    # separable form on the same 4096 planes (rows pass into a scratch field,
+    # then columns: two HBM round trips)
+    import ctypes
+    one = _lib.Plan(C.make_desc((H, W, 0), (R, R, 0), C.BorderZero, _lib.CONVOLUTION,
+                                C.NoSamplingConvolution, _lib.PLANE_BY_PLANE))
+    single_s = time_single_launch(lambda: one.run(x.data_ptr(), f.data_ptr(), y.data_ptr(), stream),
+                                  reps=100)
+    rf = torch.empty(R, device="cuda").uniform_(-1, 1, generator=gen)
+    cf = torch.empty(R, device="cuda").uniform_(-1, 1, generator=gen)
+    tmp = torch.empty_like(x)
+
+    def separable():
+        _lib.check(_lib.LIB.cct_conv_separable(H, W, P, x.data_ptr(), rf.data_ptr(), R, cf.data_ptr(), R,
+                                               _lib.BORDER_ZERO, _lib.CONVOLUTION, tmp.data_ptr(),
+                                               y.data_ptr(), ctypes.c_void_p(stream)))
+    sep_s = time_single_launch(separable, reps=10)
+    sep_bytes = 4 * 4 * P * H * W  # rows pass read + write, columns pass read + write
+    extra = {"single_plane_256x256_us": round(single_s * 1e6, 2),
+             "separable_5+5_4096x256x256": {"ms": round(sep_s * 1e3, 4),
+                                            "GB/s": round(sep_bytes / sep_s / 1e9, 1)}}
+
     byts = 4 * (2 * P * H * W + R * R)
     return {
-        "step": step, "e2e_step": e2e_step, "launch_single": step,
+        "step": step, "e2e_step": e2e_step, "launch_single": step, "extra": extra,
         "gflop_per_step": 2 * P * H * W * R * R / 1e9, "gflop_per_launch": 2 * P * H * W * R * R / 1e9,
         "bytes_per_step": byts, "e2e_gb_per_step": 4 * (2 * 64 * H * W + R * R) / 1e9,
         "h2d": 4 * (64 * H * W + R * R), "d2h": 4 * 64 * H * W,
         "metric": "GB/s", "unit": "GB/s", "precision": "fp32", "plan_algo": plan.algo,
         "config": {"workload": "plain convolve 256x256 (*) 5x5 BorderZero, 4096 planes per launch",
                    "planes": P, "H": H, "W": W, "R": R, "l2": "1 GiB input > 126 MB L2"},
-        "dtype": "f32", "keep": (plan, plan64, x, y, f, hx, hy, hf),
+        "dtype": "f32", "keep": (plan, plan64, one, x, y, f, hx, hy, hf, rf, cf, tmp),
         "kernel": "direct_tma_kernel", "bytes_per_launch": byts,
     }
 

@@ -648,15 +648,32 @@ def load_traffic(kernel):
 
 
 # ----------------------------------------------------------------------------- cpu arm
-def cpu_frame_sample(seconds_budget=10.0):
+def _timed_reps(run, seconds_budget, max_reps):
+    """Run `run` until seconds_budget has passed (at least once); (reps, seconds)."""
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > seconds_budget or reps >= max_reps:
+            return reps, el
+
+
+def _band(full, scale, least=1):
+    return max(least, min(full, int(round(full * scale))))
+
+
+def cpu_frame_sample(seconds_budget=10.0, scale=1.0):
     """Oracle (FP32 restatement of the reference kernel loop) on one image of
-    the batch, forward + backward, all host threads.  Returns (GFLOP/s,
+    the batch, forward + backward, all host threads; `scale` < 1 takes a band
+    of the image's rows (the same work per output).  Returns (GFLOP/s,
     threads, sample description)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
     import oracle as O
     rng = np.random.default_rng(2)
-    Cin, K, H, W, R = 32, 64, 64, 64, 5
+    Cin, K, W, R = 32, 64, 64, 5
+    H = _band(64, scale, 2)
     x = rng.standard_normal((Cin, H, W)).astype(np.float32)
     g = rng.standard_normal((K, H, W)).astype(np.float32)
     f = (rng.standard_normal((K * Cin, R, R)) * np.sqrt(2 / 800)).astype(np.float32)
@@ -665,48 +682,40 @@ def cpu_frame_sample(seconds_budget=10.0):
     bd = O.make_desc(H, W, R, R, planes=K, f_planes=K * Cin, batch=1, border=O.ZERO,
                      orient=O.CONV, mode=O.BACKPROJECT_REDUCE)
     threads = os.cpu_count() or 1
-    O.conv(fd, x, f, threads=threads)  # warm
-    gflop = 2 * GFLOP_FRAME / 16
-    reps, t0 = 0, time.perf_counter()
-    while True:
+    gflop = 2 * (2 * K * Cin * H * W * R * R) / 1e9
+
+    def run():
         O.conv(fd, x, f, threads=threads)
         O.conv(bd, g, f, threads=threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el > seconds_budget or reps >= 200:
-            break
-    return gflop * reps / el, threads, f"{reps} x (fwd+bwd of 1 of 16 images), {el:.1f} s"
+    reps, el = _timed_reps(run, seconds_budget, 200)
+    return gflop * reps / el, threads, f"{reps} x (fwd+bwd of {H} of 64 rows of 1 of 16 images), {el:.2f} s"
 
 
-def cpu_plain_sample(seconds_budget=10.0):
+def cpu_plain_sample(seconds_budget=10.0, scale=1.0):
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
     import oracle as O
     rng = np.random.default_rng(1)
-    P, H, W, R = 64, 256, 256, 5
+    H, W, R = 256, 256, 5
+    P = _band(64, scale)
     x = rng.uniform(-1, 1, (P, H, W)).astype(np.float32)
     f = rng.uniform(-1, 1, (R, R)).astype(np.float32)
     d = O.make_desc(H, W, R, R, planes=P, border=O.ZERO, orient=O.CONV)
     threads = os.cpu_count() or 1
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        O.conv(d, x, f, threads=threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el > seconds_budget or reps >= 200:
-            break
+    reps, el = _timed_reps(lambda: O.conv(d, x, f, threads=threads), seconds_budget, 200)
     gb = 4 * (2 * P * H * W + R * R) / 1e9
-    return gb * reps / el, threads, f"{reps} x 64 planes of 256x256, {el:.1f} s"
+    return gb * reps / el, threads, f"{reps} x {P} planes of 256x256, {el:.2f} s"
 
 
-def cpu_fft_sample(seconds_budget=10.0):
+def cpu_fft_sample(seconds_budget=10.0, scale=1.0):
     """Oracle direct convolution (the reference's loop order, FP32) of a
     band of output rows of the 2048x2048 (*) 63x63 cyclic case, all host
     threads.  GFLOP/s in the same direct-equivalent flops as the GPU line."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
     import oracle as O
-    n, k, band = 2048, 63, 64
+    n, k = 2048, 63
+    band = _band(64, scale)
     rng = np.random.default_rng(3)
     # every output point costs R*S multiply-adds whatever the border, so a
     # (band + 62) x 2048 cyclic field stands in for a band of the full field
@@ -714,40 +723,30 @@ def cpu_fft_sample(seconds_budget=10.0):
     f = gaussian_filter(k)
     d = O.make_desc(band + k - 1, n, k, k, border=O.CYCLIC, orient=O.CONV)
     threads = os.cpu_count() or 1
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        O.conv(d, x, f, threads=threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el > seconds_budget or reps >= 50:
-            break
+    reps, el = _timed_reps(lambda: O.conv(d, x, f, threads=threads), seconds_budget, 50)
     gflop = 2.0 * (band + k - 1) * n * k * k / 1e9
-    return gflop * reps / el, threads, f"{reps} x ({band + k - 1}x{n} (*) {k}x{k} cyclic), {el:.1f} s"
+    return gflop * reps / el, threads, f"{reps} x ({band + k - 1}x{n} (*) {k}x{k} cyclic), {el:.2f} s"
 
 
-def cpu_graph_sample(seconds_budget=10.0):
+def cpu_graph_sample(seconds_budget=10.0, scale=1.0):
     """Oracle FP32 projectFrameBlockReduceSum of layer 8 of the stack (28x28,
-    512 -> 512 planes, 3x3) for one sample, all host threads."""
+    512 -> 512 planes, 3x3) for one sample (or a band of its rows), all
+    host threads."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
     import oracle as O
     rng = np.random.default_rng(5)
     C = K = 512
-    H = W = 28
+    W = 28
+    H = _band(28, scale)
     x = rng.uniform(-1, 1, (C, H, W)).astype(np.float32)
     f = (rng.standard_normal((K * C, 3, 3)) * np.sqrt(2 / (C * 9))).astype(np.float32)
     d = O.make_desc(H, W, 3, 3, planes=C, f_planes=K * C, batch=1, border=O.ZERO, orient=O.XCORR,
                     mode=O.PROJECT_REDUCE)
     threads = os.cpu_count() or 1
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        O.conv(d, x, f, threads=threads)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el > seconds_budget or reps >= 100:
-            break
+    reps, el = _timed_reps(lambda: O.conv(d, x, f, threads=threads), seconds_budget, 100)
     gflop = 2.0 * K * C * H * W * 9 / 1e9
-    return gflop * reps / el, threads, f"{reps} x layer 8 of one sample (28x28, 512->512, 3x3), {el:.1f} s"
+    return gflop * reps / el, threads, f"{reps} x layer 8 of one sample ({H} of 28 rows, 512->512, 3x3), {el:.2f} s"
 
 
 # ----------------------------------------------------------------------------- main
@@ -761,13 +760,24 @@ def run_reference(args):
         return 0
     fn = {"frame": cpu_frame_sample, "plain": cpu_plain_sample, "fft": cpu_fft_sample,
           "graph": cpu_graph_sample}[args.workload]
+    # The whole run stays within about two minutes: at most 40 timed samples
+    # (the median is reported), each given an equal share of the budget; a
+    # sample that would overrun its share shrinks to a band of the workload
+    # (the same work per output).
+    samples = max(1, min(args.steps, 40))
+    step_budget = min(2.0, 100.0 / samples)
+    t0 = time.perf_counter()
+    fn(seconds_budget=0.0)
+    unit = time.perf_counter() - t0
+    scale = min(1.0, step_budget / max(unit, 1e-9))
     per = []
-    for _ in range(max(args.warmup, 0)):
-        fn(seconds_budget=1.0)
-    for _ in range(args.steps):
-        v, threads, sample = fn(seconds_budget=2.0)
+    for _ in range(min(max(args.warmup, 0), 3)):
+        fn(seconds_budget=0.0, scale=scale)
+    for _ in range(samples):
+        v, threads, sample = fn(seconds_budget=step_budget, scale=scale)
         per.append(v)
     value = statistics.median(per)
+    sample = f"median of {samples} samples, last: {sample}"
     unit = "GB/s" if args.workload == "plain" else "GFLOP/s"
     cfg = {"workload": {
         "frame": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 K=64 64x64 5x5 "

@@ -227,6 +227,37 @@ def test_separable_bitwise(border, orient):
     assert bitwise_equal(y.cpu().numpy(), O.separable(x, row, col, border, orient))
 
 
+# filter lengths with compiled kernels (<= 9: TMA-staged under BorderZero when
+# the width is a multiple of 4, register-window otherwise), the generic fused
+# tile (longer) and the two-pass form (> 96 KB tile); fields smaller than,
+# equal to and a few tiles larger than one tile, ragged in rows and columns
+@pytest.mark.parametrize("rlen,clen", [(1, 1), (3, 9), (9, 3), (5, 5), (7, 1), (11, 13), (33, 17),
+                                       (301, 3), (3, 301)])
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 1, 4), (2, 32, 64), (2, 97, 150), (2, 97, 152),
+                                   (1, 257, 196)])
+def test_separable_lengths(rlen, clen, shape):
+    import cctconv as C
+    rng = np.random.default_rng(rlen * 100 + clen)
+    x = rng.uniform(-1, 1, shape).astype(np.float32)
+    row = rng.uniform(-1, 1, rlen).astype(np.float32)
+    col = rng.uniform(-1, 1, clen).astype(np.float32)
+    xd, rd, cd = (torch.from_numpy(a).cuda() for a in (x, row, col))
+    for border, pol in [(O.ZERO, C.BorderZero), (O.CLAMP, C.BorderClamp), (O.CYCLIC, C.BorderCyclic)]:
+        for orient, fn in [(O.XCORR, C.crossCorrelateSeparable), (O.CONV, C.convolveSeparable)]:
+            y = fn(xd, rd, cd, pol)
+            torch.cuda.synchronize()
+            assert bitwise_equal(y.cpu().numpy(), O.separable(x, row, col, border, orient)), \
+                (rlen, clen, shape, border, orient)
+
+
+def test_separable_even_length_rejected():
+    """Filters must be of odd size (ConvolveRows2DHyperKernel.scala:218-219)."""
+    import cctconv as C
+    x = torch.zeros((8, 8), device="cuda")
+    with pytest.raises(ValueError, match="odd"):
+        C.convolveSeparable(x, torch.ones(4, device="cuda"), torch.ones(3, device="cuda"), C.BorderZero)
+
+
 def test_edge_cases():
     rng = np.random.default_rng(8)
     # 1x1 field, filter larger than the field (centred borders), prime sizes

@@ -12,8 +12,16 @@ Names, argument meaning and error behaviour follow the reference's
   backProjectFrameBlockReduceSum(...)                                  :1450
 
 Fields are CUDA float32 tensors in cct-core's planar layout: ``(cols,)`` is a
-1-D ScalarField, ``(rows, cols)`` a 2-D ScalarField and ``(planes, rows,
-cols)`` a 2-D VectorField (tensor planes first, each plane row-major).
+1-D ScalarField, ``(rows, cols)`` a 2-D ScalarField, ``(planes, rows,
+cols)`` a 2-D VectorField (tensor planes first, each plane row-major) and
+``(size, size, rows, cols)`` a 2-D MatrixField of size x size matrices (tensor
+elements first).  A ColorField is a CUDA uint8 tensor ``(rows, cols, 4)``:
+RGBA bytes per pixel, the reference's UNORM_INT8 image.
+
+convolve / crossCorrelate also take the two special operand pairs of
+CogFunctionAPI.convolveInternal (:1128-1238): a ScalarField with a MatrixField
+filter (ScalarMatrixConvolve2D, :1209-1216) and a ColorField image
+(DynamicConvolutionGenerator.scala:89-106).
 torch only supplies device memory and the current stream; every convolution
 runs in libcctconv's CUDA kernels.  Illegal arguments raise ``ValueError``
 with the reference's message (the reference throws from ``require``).
@@ -159,14 +167,87 @@ def _run(field, filt, border, orientation, sampling, mode, batch, precision=_lib
     return y
 
 
+def _is_color_field(t):
+    return isinstance(t, torch.Tensor) and t.dtype == torch.uint8 and t.dim() == 3 and t.shape[2] == 4
+
+
+def _is_matrix_field(t):
+    return isinstance(t, torch.Tensor) and t.dim() == 4
+
+
+def _scalar_matrix(field, matrices, border, orientation, sampling):
+    """ScalarField (*) MatrixField -> VectorField of one plane per matrix,
+    plane index row * matrix_cols + col (ScalarMatrixConvolve2DHyperKernel)."""
+    if not field.is_cuda or not matrices.is_cuda:
+        raise ValueError("fields must live on a CUDA device")
+    if matrices.dtype != torch.float32:
+        raise TypeError("filter must be float32")
+    if field.dim() != 2:
+        raise ValueError("a MatrixField filter needs a 2-D ScalarField input")
+    rows, cols, _ = _shape_of(field, "field")
+    size, size2, mrows, mcols = matrices.shape
+    if size != size2:
+        raise ValueError("matrix in field must be square")
+    x, m = field.contiguous(), matrices.contiguous()
+    y = torch.empty((mrows * mcols, rows, cols), device=field.device, dtype=torch.float32)
+    st = _lib.LIB.cct_conv_scalar_matrix(rows, cols, x.data_ptr(), m.data_ptr(), mrows, mcols, size,
+                                         border.code, orientation, sampling.code, sampling.step,
+                                         y.data_ptr(),
+                                         ctypes.c_void_p(torch.cuda.current_stream(field.device).cuda_stream))
+    if st == _lib.EINVAL:
+        raise ValueError(_lib.LIB.cct_last_error_string().decode())
+    _lib.check(st)
+    return y
+
+
+_COLOR_PLANS = {}
+
+
+def _color(field, filt, border, orientation, sampling, algo):
+    """ColorField convolution: red, green, blue each convolved with the
+    scalar filter, merged back into a ColorField of the output shape."""
+    if not field.is_cuda or not filt.is_cuda:
+        raise ValueError("fields must live on a CUDA device")
+    rows, cols = field.shape[0], field.shape[1]
+    frows, fcols, fplanes = _shape_of(filt, "filter")
+    if fplanes != 0 or filt.dim() != 2:
+        raise ValueError("a ColorField is convolved with a 2-D ScalarField filter")
+    desc = make_desc((rows, cols, 0), (frows, fcols, 0), border, orientation, sampling,
+                     _lib.PLANE_BY_PLANE, algo=algo)
+    try:
+        orows, ocols, _ = _lib.output_shape(desc)
+    except CctError as e:
+        raise ValueError(str(e)) from None
+    dev = field.device.index
+    key = (dev, desc.key())
+    with _PLANS_LOCK:
+        plan = _COLOR_PLANS.get(key)
+        if plan is None:
+            with torch.cuda.device(dev):
+                plan = _lib.ColorPlan(desc)
+            _COLOR_PLANS[key] = plan
+    x, f = field.contiguous(), filt.contiguous()
+    y = torch.empty((orows, ocols, 4), device=field.device, dtype=torch.uint8)
+    plan.run(x.data_ptr(), f.data_ptr(), y.data_ptr(), torch.cuda.current_stream(field.device).cuda_stream)
+    return y
+
+
 def crossCorrelate(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
                    fftUse=UseFFTWhenBest):
+    if _is_color_field(field):
+        return _color(field, filter, borderPolicy, _lib.CROSS_CORRELATION, samplingPolicy, fftUse.code)
+    if _is_matrix_field(filter):
+        return _scalar_matrix(field, filter, borderPolicy, _lib.CROSS_CORRELATION, samplingPolicy)
     return _run(field, filter, borderPolicy, _lib.CROSS_CORRELATION, samplingPolicy,
                 _lib.PLANE_BY_PLANE, 1, algo=fftUse.code)
 
 
 def convolve(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
              fftUse=UseFFTWhenBest):
+    if _is_color_field(field):
+        return _color(field, filter, borderPolicy, _lib.CONVOLUTION, samplingPolicy, fftUse.code)
+    if _is_matrix_field(filter):
+        return _scalar_matrix(field, filter, borderPolicy, _lib.CONVOLUTION, samplingPolicy)
     return _run(field, filter, borderPolicy, _lib.CONVOLUTION, samplingPolicy,
                 _lib.PLANE_BY_PLANE, 1, algo=fftUse.code)
 

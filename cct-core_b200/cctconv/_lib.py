@@ -87,6 +87,11 @@ SIGNATURES = {
     "cct_conv_run_host": (_I, [_P, _P, _P, _P, _P]),
     "cct_conv_separable": (_I, [_I32, _I32, _I32, _P, _P, _I32, _P, _I32, _I32, _I32, _P, _P, _P]),
     "cct_conv_run_noalloc": (_I, [ctypes.POINTER(ConvDesc), _P, _P, _P, _P]),
+    "cct_conv_scalar_matrix": (_I, [_I32, _I32, _P, _P, _I32, _I32, _I32, _I32, _I32, _I32, _I32, _P, _P]),
+    "cct_color_plan_create": (_I, [ctypes.POINTER(ConvDesc), ctypes.POINTER(_P)]),
+    "cct_color_plan_set_static_filter": (_I, [_P, _P]),
+    "cct_color_run": (_I, [_P, _P, _P, _P, _P]),
+    "cct_color_plan_destroy": (_I, [_P]),
     "cct_graph_create": (_I, [ctypes.POINTER(ConvDesc), _I32, ctypes.POINTER(_P)]),
     "cct_graph_destroy": (_I, [_P]),
     "cct_graph_set_filter": (_I, [_P, _I32, _P]),
@@ -184,6 +189,36 @@ class Plan:
     def close(self):
         if self.handle:
             LIB.cct_conv_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ColorPlan:
+    """Owning wrapper of a cct_color_plan (colour-field convolution: RGBA8 in
+    and out, the three colour planes convolved with one scalar filter)."""
+
+    def __init__(self, desc):
+        self.desc = desc
+        self.shape = output_shape(desc)
+        h = ctypes.c_void_p()
+        check(LIB.cct_color_plan_create(ctypes.byref(desc), ctypes.byref(h)))
+        self.handle = h
+
+    def set_static_filter(self, host_ptr):
+        check(LIB.cct_color_plan_set_static_filter(self.handle, ctypes.c_void_p(host_ptr)))
+
+    def run(self, x_ptr, f_ptr, y_ptr, stream=0):
+        check(LIB.cct_color_run(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(f_ptr),
+                                ctypes.c_void_p(y_ptr), ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self.handle:
+            LIB.cct_color_plan_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -477,6 +477,27 @@ int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes, const float *
                           tmp, y, (cudaStream_t)stream);
 }
 
+int cct_conv_scalar_matrix(int32_t rows, int32_t cols, const float *image, const float *matrices,
+                           int32_t matrix_rows, int32_t matrix_cols, int32_t size, int32_t border,
+                           int32_t orientation, int32_t sampling, int32_t step, float *out, void *stream) {
+  // ScalarMatrixConvolve2DHyperKernel.apply (ScalarMatrixConvolve2DHyperKernel.scala:118-152)
+  if (border == CCT_BORDER_FULL) return set_error(CCT_EINVAL, "unsupported: BorderFull");
+  if (border == CCT_BORDER_VALID) return set_error(CCT_EINVAL, "unsupported: BorderValid");
+  if (border != CCT_BORDER_ZERO && border != CCT_BORDER_CLAMP && border != CCT_BORDER_CYCLIC)
+    return set_error(CCT_EINVAL, "bad border policy %d", border);
+  // CogFunctionAPI.scala:1139-1143: step-1 sampling is NoSampling
+  if (sampling != CCT_SAMPLE_NONE && !(step == 1 && (sampling == CCT_SAMPLE_DOWN || sampling == CCT_SAMPLE_UP)))
+    return set_error(CCT_EINVAL, "sampling not supported yet");
+  if (orientation != CCT_CROSS_CORRELATION) return set_error(CCT_EINVAL, "convolution not supported yet");
+  if (rows < 1 || cols < 1 || matrix_rows < 1 || matrix_cols < 1 || size < 1)
+    return set_error(CCT_EINVAL, "field, matrix field and matrix sizes must be positive");
+  if (size % 2 != 1) return set_error(CCT_EINVAL, "matrix in field must have odd size");
+  if (!image || !matrices || !out) return set_error(CCT_EINVAL, "null image, matrix or output pointer");
+  const long long L = (long long)matrix_rows * matrix_cols;
+  if (L > (1 << 24)) return set_error(CCT_ENOTSUP, "scalar-matrix convolution: too many matrices");
+  return launch_scalar_matrix(rows, cols, image, matrices, (int)L, size, border, out, (cudaStream_t)stream);
+}
+
 int cct_malloc(void **ptr, size_t bytes) {
   if (!ptr) return set_error(CCT_EINVAL, "null pointer argument");
   return check_cuda(cudaMalloc(ptr, bytes), "cudaMalloc");

@@ -108,6 +108,8 @@ int launch_fa_f32(const ConvGeom &g, const float *x, const float *f, float *y, f
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);
+int launch_scalar_matrix(int rows, int cols, const float *x, const float *mats, int L, int size, int border,
+                         float *y, cudaStream_t stream);
 int launch_separable(int rows, int cols, int planes, const float *x,
                      const float *rf, int rlen, const float *cf, int clen,
                      int border, int orient, float *tmp, float *y,

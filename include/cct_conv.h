@@ -157,6 +157,46 @@ int cct_conv_separable(int32_t rows, int32_t cols, int32_t planes,
                        int32_t col_len, int32_t border, int32_t orientation,
                        float *tmp, float *out, void *stream);
 
+/* A ScalarField cross-correlated with every matrix of a MatrixField: the form
+ * api/CogFunctionAPI.scala:1209-1216 selects for convolve/crossCorrelate of a
+ * scalar field with a matrix field; replaces
+ * hyperkernels/ScalarMatrixConvolve2DHyperKernel.scala:43-160.
+ *   image     rows x cols
+ *   matrices  a matrix field of matrix_rows x matrix_cols points, each a
+ *             size x size matrix, stored tensor-element-major: element
+ *             (r, c) of matrix p = row * matrix_cols + col is at
+ *             matrices[(r * size + c) * matrix_rows * matrix_cols + p]
+ *   out       matrix_rows * matrix_cols planes of rows x cols (a vector field)
+ * Each output is one fused multiply-add chain from 0 over the taps in
+ * row-major order, as the reference kernel sums.  The reference's
+ * restrictions and messages hold: BorderZero / Clamp / Cyclic, no sampling
+ * (step 1 counts as none), cross-correlation only, odd size. */
+int cct_conv_scalar_matrix(int32_t rows, int32_t cols, const float *image,
+                           const float *matrices, int32_t matrix_rows,
+                           int32_t matrix_cols, int32_t size, int32_t border,
+                           int32_t orientation, int32_t sampling, int32_t step,
+                           float *out, void *stream);
+
+/* Colour-field convolution (generator/DynamicConvolutionGenerator.scala:
+ * 89-106).  A ColorField is an RGBA8 image, 4 bytes per pixel, as the
+ * reference's UNORM_INT8 image buffer (platform/opencl/OpenCLBuffer.scala:
+ * 135-136); alpha is ignored on input.  Each of red, green, blue (byte / 255)
+ * is convolved with the one scalar filter as `desc` describes: the image
+ * shape, filter shape, border, orientation, sampling and algorithm of a
+ * plane-by-plane convolution (image_planes 0 or 1, filter_planes 0 or 1,
+ * FP32).  The result is an RGBA8 colour field of the output shape
+ * (cct_conv_output_shape of desc) with each channel saturate(v * 255)
+ * rounded half to even and alpha 255, as CreateColorFieldHyperKernel writes
+ * (hyperkernels/CreateColorFieldHyperKernel.scala:35-40).  Image and output
+ * must be 4-byte aligned device pointers; the plan owns six planes of
+ * workspace. */
+typedef struct cct_color_plan cct_color_plan;
+int cct_color_plan_create(const cct_conv_desc *desc, cct_color_plan **plan);
+int cct_color_plan_set_static_filter(cct_color_plan *plan, const float *host_filter);
+int cct_color_run(const cct_color_plan *plan, const uint8_t *image,
+                  const float *filter, uint8_t *out, void *stream);
+int cct_color_plan_destroy(cct_color_plan *plan);
+
 /* Allocation-free variant of the BF16X3 BlockReduceSum frame convolution (no
  * counterpart in the reference, which always lets its runtime own device
  * buffers).  For callers that cannot call cudaMalloc when they convolve:

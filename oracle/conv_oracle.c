@@ -343,3 +343,60 @@ int oracle_separable_f32(int rows, int cols, int planes, const float *x,
   free(tmp);
   return 0;
 }
+
+/* Scalar field (*) matrix field (ScalarMatrixConvolve2DHyperKernel.scala:
+ * 59-85; reached from CogFunctionAPI.scala:1209-1216 when a scalar field is
+ * convolved with a matrix field).  Output plane p = row * mcols + col is the
+ * cross-correlation of x with the size x size matrix at (row, col), summed as
+ * ONE fused multiply-add chain from 0 over the taps in row-major order (the
+ * kernel's `sum += inputPixel * filterElement`, contracted under
+ * -cl-mad-enable), with halo size / 2 and the border's index rule.  The
+ * matrix field is stored tensor-element-major: element (r, c) of matrix p at
+ * mats[(r * size + c) * (mrows * mcols) + p]. */
+int oracle_scalar_matrix_f32(int rows, int cols, const float *x, const float *mats,
+                             int mrows, int mcols, int size, int border, float *y) {
+  if (border != OR_ZERO && border != OR_CLAMP && border != OR_CYCLIC) return 1;
+  if (size < 1 || size % 2 == 0 || mrows < 1 || mcols < 1) return 1;
+  const int L = mrows * mcols, h = size / 2;
+  const size_t page = (size_t)rows * cols;
+  for (int p = 0; p < L; p++)
+    for (int i = 0; i < rows; i++)
+      for (int j = 0; j < cols; j++) {
+        float sum = 0.0f;
+        for (int r = 0; r < size; r++) {
+          const int si = border_index(border, i - h + r, rows);
+          for (int c = 0; c < size; c++) {
+            const int sj = border_index(border, j - h + c, cols);
+            const float v = (si < 0 || sj < 0) ? 0.0f : x[(size_t)si * cols + sj];
+            sum = fmaf(v, mats[(size_t)(r * size + c) * L + p], sum);
+          }
+        }
+        y[(size_t)p * page + (size_t)i * cols + j] = sum;
+      }
+  return 0;
+}
+
+/* ColorField planes (ColorPlaneHyperKernel.scala:38-44 reads a pixel of the
+ * RGBA UNORM_INT8 image, OpenCLBuffer.scala:135-136): channel byte c reads
+ * as c / 255 (the OpenCL conversion for UNORM_INT8, rounded to nearest).
+ * planes[k * n + i] = channel k (red, green, blue) of pixel i. */
+void oracle_color_unpack(int n, const unsigned char *rgba, float *planes) {
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) planes[(size_t)k * n + i] = (float)rgba[4 * (size_t)i + k] / 255.0f;
+}
+
+/* MergeColorPlanes (CreateColorFieldHyperKernel.scala:35-40) writes
+ * (red, green, blue, 1) to the UNORM_INT8 image: per channel
+ * convert_uchar_sat_rte(v * 255.0f) (NaN -> 0, saturate to [0, 255], round
+ * half to even). */
+void oracle_color_pack(int n, const float *planes, unsigned char *rgba) {
+  for (int i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) {
+      const float v = planes[(size_t)k * n + i] * 255.0f;
+      float q = v > 0.0f ? v : 0.0f; /* NaN -> 0 */
+      if (q > 255.0f) q = 255.0f;
+      rgba[4 * (size_t)i + k] = (unsigned char)nearbyintf(q);
+    }
+    rgba[4 * (size_t)i + 3] = 255;
+  }
+}

@@ -61,6 +61,19 @@ int oracle_separable_f32(int rows, int cols, int planes, const float *x,
                          const float *row_f, int row_len, const float *col_f,
                          int col_len, int border, int orient, float *y);
 
+/* Scalar field cross-correlated with every matrix of a matrix field
+ * (ScalarMatrixConvolve2DHyperKernel.scala): one output plane per matrix,
+ * one fma chain per output over the taps in row-major order.  border in
+ * {ZERO, CLAMP, CYCLIC}; size odd.  mats is tensor-element-major. */
+int oracle_scalar_matrix_f32(int rows, int cols, const float *x, const float *mats,
+                             int mrows, int mcols, int size, int border, float *y);
+
+/* ColorField <-> planes: RGBA8 pixels (alpha ignored on read, 255 on write)
+ * to three float planes (byte / 255) and back (saturate, x 255, round half to
+ * even), as the OpenCL UNORM_INT8 image conversions. */
+void oracle_color_unpack(int n, const unsigned char *rgba, float *planes);
+void oracle_color_pack(int n, const float *planes, unsigned char *rgba);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,11 @@ def lib():
                                            P(ctypes.c_float), P(ctypes.c_float), ctypes.c_int,
                                            P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
                                            ctypes.c_int, P(ctypes.c_float)]
+        L.oracle_scalar_matrix_f32.argtypes = [ctypes.c_int, ctypes.c_int, P(ctypes.c_float),
+                                               P(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, ctypes.c_int, P(ctypes.c_float)]
+        L.oracle_color_unpack.argtypes = [ctypes.c_int, P(ctypes.c_ubyte), P(ctypes.c_float)]
+        L.oracle_color_pack.argtypes = [ctypes.c_int, P(ctypes.c_float), P(ctypes.c_ubyte)]
         _LIB = L
     return _LIB
 
@@ -151,3 +156,50 @@ def poor_float_equal(a, b):
 if __name__ == "__main__":
     build()
     print(os.path.join(_HERE, "liboracle.so"))
+
+
+def scalar_matrix(x, mats, border):
+    """Scalar field (rows, cols) cross-correlated with a matrix field given as
+    (size, size, mrows, mcols) (tensor-element-major, as stored); returns
+    (mrows * mcols, rows, cols)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    mats = np.ascontiguousarray(mats, dtype=np.float32)
+    size, size2, mr, mc = mats.shape
+    assert size == size2
+    rows, cols = x.shape
+    y = np.zeros((mr * mc, rows, cols), dtype=np.float32)
+    P = ctypes.POINTER(ctypes.c_float)
+    rc = lib().oracle_scalar_matrix_f32(rows, cols, x.ctypes.data_as(P), mats.ctypes.data_as(P), mr, mc,
+                                        size, border, y.ctypes.data_as(P))
+    if rc:
+        raise ValueError("oracle rejected scalar-matrix arguments")
+    return y
+
+
+def color_unpack(rgba):
+    """(rows, cols, 4) uint8 -> (3, rows, cols) float32 planes (byte / 255)."""
+    rgba = np.ascontiguousarray(rgba, dtype=np.uint8)
+    rows, cols, _ = rgba.shape
+    out = np.zeros((3, rows, cols), dtype=np.float32)
+    lib().oracle_color_unpack(rows * cols, rgba.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+    return out
+
+
+def color_pack(planes):
+    """(3, rows, cols) float32 -> (rows, cols, 4) uint8, alpha 255."""
+    planes = np.ascontiguousarray(planes, dtype=np.float32)
+    _, rows, cols = planes.shape
+    out = np.zeros((rows, cols, 4), dtype=np.uint8)
+    lib().oracle_color_pack(rows * cols, planes.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+    return out
+
+
+def color_conv(desc, rgba, f):
+    """ColorField convolution (DynamicConvolutionGenerator.scala:89-106): the
+    red, green and blue planes each convolved with the scalar filter as
+    `desc` describes (its plane counts are ignored), then merged."""
+    d = OracleDesc(*[getattr(desc, n) for n, _ in OracleDesc._fields_])
+    d.planes, d.f_planes = 3, 0
+    return color_pack(conv(d, color_unpack(rgba), f))

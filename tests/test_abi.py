@@ -144,3 +144,34 @@ def test_server_and_graph_need_a_device():
     bad.slots = 9
     rc = _lib.LIB.cct_server_create(ctypes.byref(bad), ctypes.byref(h))
     assert rc in (_lib.EINVAL, _lib.ENODEV)
+
+
+@pytest.mark.parametrize("border,orient,sampling,step,size,msg", [
+    (_lib.BORDER_FULL, _lib.CROSS_CORRELATION, _lib.SAMPLE_NONE, 1, 3, "unsupported: BorderFull"),
+    (_lib.BORDER_VALID, _lib.CROSS_CORRELATION, _lib.SAMPLE_NONE, 1, 3, "unsupported: BorderValid"),
+    (_lib.BORDER_ZERO, _lib.CONVOLUTION, _lib.SAMPLE_NONE, 1, 3, "convolution not supported yet"),
+    (_lib.BORDER_CLAMP, _lib.CROSS_CORRELATION, _lib.SAMPLE_DOWN, 2, 3, "sampling not supported yet"),
+    (_lib.BORDER_CYCLIC, _lib.CROSS_CORRELATION, _lib.SAMPLE_UP, 3, 3, "sampling not supported yet"),
+    (_lib.BORDER_ZERO, _lib.CROSS_CORRELATION, _lib.SAMPLE_NONE, 1, 4, "odd size"),
+])
+def test_scalar_matrix_reference_restrictions(border, orient, sampling, step, size, msg):
+    """ScalarMatrixConvolve2DHyperKernel.scala:118-152 rejects these before
+    any device work."""
+    rc = _lib.LIB.cct_conv_scalar_matrix(8, 8, 16, 16, 2, 2, size, border, orient, sampling, step, 16, None)
+    assert rc == _lib.EINVAL
+    assert msg in _lib.LIB.cct_last_error_string().decode()
+
+
+def test_color_plan_descriptor_checks():
+    h = ctypes.c_void_p()
+    for kw, msg in [(dict(image_planes=3), "one colour field"), (dict(filter_planes=2), "scalar filter"),
+                    (dict(vector_mode=_lib.PROJECT_FRAME), "plane by plane"),
+                    (dict(precision=_lib.PREC_BF16X3), "FP32")]:
+        d = _lib.new_desc(image_rows=8, image_cols=8, filter_rows=3, filter_cols=3, **kw)
+        assert _lib.LIB.cct_color_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.EINVAL
+        assert msg in _lib.LIB.cct_last_error_string().decode()
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    d = _lib.new_desc(image_rows=8, image_cols=8, filter_rows=3, filter_cols=3)
+    assert _lib.LIB.cct_color_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.ENODEV

@@ -323,3 +323,87 @@ def test_filter_adjoint_shape_rules():
     assert shape(O.FILTER_ADJOINT, 6, 8, 2, O.UP, 2) == (40 - 16 + 1, 25, 24)
     with pytest.raises(ValueError):
         shape(O.FILTER_ADJOINT, 6, 7, 2)
+
+
+# ---- ScalarMatrixConvolve2D and colour fields -----------------------------
+
+def _np_border(border, v, n):
+    if border == O.CLAMP:
+        return min(max(v, 0), n - 1)
+    if border == O.CYCLIC:
+        return v % n
+    return v if 0 <= v < n else -1
+
+
+@pytest.mark.parametrize("border", [O.ZERO, O.CLAMP, O.CYCLIC])
+def test_scalar_matrix_oracle_restates_the_kernel_loop(border):
+    """One fma chain per output over the taps in row-major order
+    (ScalarMatrixConvolve2DHyperKernel.scala:59-85), output plane
+    row * matrix_cols + col; checked against a float32 loop written here."""
+    rng = np.random.default_rng(31)
+    rows, cols, size, mr, mc = 6, 7, 3, 2, 3
+    x = rng.uniform(-1, 1, (rows, cols)).astype(np.float32)
+    mats = rng.uniform(-1, 1, (size, size, mr, mc)).astype(np.float32)
+    y = O.scalar_matrix(x, mats, border)
+    h = size // 2
+    for p in range(mr * mc):
+        for i in range(rows):
+            for j in range(cols):
+                s = np.float32(0)
+                for r in range(size):
+                    for c in range(size):
+                        si, sj = _np_border(border, i - h + r, rows), _np_border(border, j - h + c, cols)
+                        v = np.float32(0) if si < 0 or sj < 0 else x[si, sj]
+                        # fma in float64 is exact for a float32 product, then one rounding
+                        s = np.float32(np.float64(v) * np.float64(mats[r, c, p // mc, p % mc]) + np.float64(s))
+                assert y[p, i, j] == s, (p, i, j)
+
+
+def test_scalar_matrix_matches_reference_test_by_convolve_of_flipped_matrices():
+    """StaticConvolutionSpec.scala:2361-2393: crossCorrelate(scalar, matrixField,
+    BorderClamp) ~== the vector field of convolve(scalar, matrix.flip,
+    BorderClamp), row-major over the matrix field (4x5 field, 2x3 matrices of
+    3x3)."""
+    rng = np.random.default_rng(32)
+    x = rng.random((4, 5)).astype(np.float32)
+    mats = rng.random((3, 3, 2, 3)).astype(np.float32)
+    y = O.scalar_matrix(x, mats, O.CLAMP)
+    expected = np.stack([O.conv(O.make_desc(4, 5, 3, 3, border=O.CLAMP, orient=O.CONV), x,
+                                np.ascontiguousarray(mats[::-1, ::-1, r, c]))[0]
+                         for r in range(2) for c in range(3)])
+    assert ref_field_approx_equal(y, expected)
+
+
+def test_color_conversions_known_answers():
+    """UNORM_INT8 read: byte / 255; MergeColorPlanes write:
+    convert_uchar_sat_rte(v * 255) with alpha 255."""
+    rgba = np.array([[[0, 1, 128, 7], [254, 255, 51, 0]]], dtype=np.uint8)
+    planes = O.color_unpack(rgba)
+    assert planes.shape == (3, 1, 2)
+    for k in range(3):
+        for j in range(2):
+            assert planes[k, 0, j] == np.float32(rgba[0, j, k]) / np.float32(255)
+    back = O.color_pack(planes)
+    assert np.array_equal(back[..., :3], rgba[..., :3]) and np.all(back[..., 3] == 255)
+    v = np.array([np.nan, -0.5, 0.0, 2.5 / 255, 3.5 / 255, 0.999, 1.0, 7.0], dtype=np.float32)
+    got = O.color_pack(np.stack([v[None, :]] * 3))[0, :, 0]
+    want = []
+    for f in v:
+        s = np.float32(f) * np.float32(255)
+        s = 0.0 if not s > 0 else min(float(s), 255.0)
+        want.append(int(np.rint(s)))  # numpy rounds half to even
+    assert list(got) == want
+    assert list(got[:3]) == [0, 0, 0] and got[-1] == 255
+
+
+def test_color_conv_is_three_plane_convs():
+    rng = np.random.default_rng(33)
+    rgba = rng.integers(0, 256, (9, 11, 4), dtype=np.uint8)
+    f = rng.uniform(-0.3, 0.3, (3, 3)).astype(np.float32)
+    d = O.make_desc(9, 11, 3, 3, border=O.CYCLIC, orient=O.CONV)
+    out = O.color_conv(d, rgba, f)
+    planes = O.color_unpack(rgba)
+    for k in range(3):
+        yk = O.conv(d, planes[k], f)[0]
+        assert np.array_equal(out[..., k], O.color_pack(np.stack([yk] * 3))[..., 0])
+    assert np.all(out[..., 3] == 255)

@@ -134,3 +134,26 @@ def test_tc_repeatable():
     a = run_tc(od, x, f)
     b = run_tc(od, x, f)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("mode,relu", [(O.PROJECT_REDUCE, False), (O.PROJECT_REDUCE, True),
+                                       (O.BACKPROJECT_REDUCE, False)])
+def test_tc_partial_last_wave_two_plane_blocks(mode, relu):
+    """176 tiles on 148 SMs (a partial second wave), 64 input planes as two
+    32-plane halo blocks of 9 taps each: within tolerance of FP64, ReLU
+    applied once, and bit-identical run to run."""
+    rng = np.random.default_rng(91 + mode)
+    H, W, C, K, B, R = 32, 64, 64, 48, 11, 3
+    if mode == O.PROJECT_REDUCE:
+        planes, orient = B * C, O.XCORR
+    else:
+        planes, orient = B * K, O.CONV
+    od = O.make_desc(H, W, R, R, planes=planes, f_planes=K * C, batch=B, border=O.ZERO,
+                     orient=orient, mode=mode)
+    x = rng.standard_normal((planes, H, W)).astype(np.float32)
+    f = rng.standard_normal((K * C, R, R)).astype(np.float32)
+    flags = _lib.FLAG_RELU if relu else 0
+    a = run_tc(od, x, f, flags=flags)
+    check(a, od, x, f, relu=relu)
+    b = run_tc(od, x, f, flags=flags)
+    assert np.array_equal(a, b)

@@ -100,6 +100,12 @@ SIGNATURES = {
     "cct_graph_step_host": (_I, [_P, _P, _P, _P]),
     "cct_graph_time": (ctypes.c_int64, [_P]),
     "cct_graph_reset": (_I, [_P]),
+    "cct_graph_save": (_I, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_graph_restore": (_I, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "cct_conv_plan_save": (_I, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_conv_plan_restore": (_I, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "cct_record_describe": (_I, [_P, ctypes.c_size_t, _PI32, _PI32, ctypes.POINTER(ctypes.c_int64),
+                                 ctypes.POINTER(ConvDesc), _I32]),
     "cct_server_config_init": (None, [ctypes.POINTER(ServerConfig)]),
     "cct_serve_request_init": (None, [ctypes.POINTER(ServeRequest)]),
     "cct_server_create": (_I, [ctypes.POINTER(ServerConfig), ctypes.POINTER(_P)]),
@@ -162,18 +168,57 @@ def output_shape(desc):
     return r.value, c.value, p.value
 
 
+def _save_record(fn, handle):
+    """Checkpoint record of a plan or graph as a numpy uint32 array."""
+    import numpy as np
+    n = ctypes.c_size_t()
+    check(fn(handle, None, 0, ctypes.byref(n)))
+    words = np.zeros(n.value, dtype=np.uint32)
+    check(fn(handle, ctypes.c_void_p(words.ctypes.data), n.value, ctypes.byref(n)))
+    return words
+
+
+def describe_record(words):
+    """(kind, layer descriptors, step count) of a checkpoint record; kind 1
+    is a plan, 2 a graph.  Needs no device."""
+    import numpy as np
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    kind, n, t = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+    check(LIB.cct_record_describe(ctypes.c_void_p(w.ctypes.data), w.size, ctypes.byref(kind),
+                                  ctypes.byref(n), ctypes.byref(t), None, 0))
+    descs = (ConvDesc * n.value)()
+    check(LIB.cct_record_describe(ctypes.c_void_p(w.ctypes.data), w.size, None, None, None, descs, n.value))
+    return kind.value, list(descs), t.value
+
+
 class Plan:
     """Owning wrapper of a cct_conv_plan."""
 
-    def __init__(self, desc):
+    def __init__(self, desc, _handle=None):
         self.desc = desc
         self.shape = output_shape(desc)
         h = ctypes.c_void_p()
-        check(LIB.cct_conv_plan_create(ctypes.byref(desc), ctypes.byref(h)))
+        if _handle is None:
+            check(LIB.cct_conv_plan_create(ctypes.byref(desc), ctypes.byref(h)))
+        else:
+            h = _handle
         self.handle = h
         a = ctypes.c_int32()
         check(LIB.cct_conv_plan_algo(h, ctypes.byref(a)))
         self.algo = a.value
+
+    def save(self):
+        """Checkpoint record (numpy uint32 words): descriptor + constant filter."""
+        return _save_record(LIB.cct_conv_plan_save, self.handle)
+
+    @classmethod
+    def restore(cls, words):
+        import numpy as np
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        check(LIB.cct_conv_plan_restore(ctypes.c_void_p(w.ctypes.data), w.size, ctypes.byref(h)))
+        _, descs, _ = describe_record(w)
+        return cls(descs[0], _handle=h)
 
     def set_static_filter(self, host_ptr):
         check(LIB.cct_conv_plan_set_static_filter(self.handle, ctypes.c_void_p(host_ptr)))
@@ -232,10 +277,13 @@ class Graph:
     """Owning wrapper of a cct_graph: a chain of convolution layers stepped
     as one captured launch sequence."""
 
-    def __init__(self, descs):
-        arr = (ConvDesc * len(descs))(*descs)
-        h = ctypes.c_void_p()
-        check(LIB.cct_graph_create(arr, len(descs), ctypes.byref(h)))
+    def __init__(self, descs, _handle=None):
+        if _handle is None:
+            arr = (ConvDesc * len(descs))(*descs)
+            h = ctypes.c_void_p()
+            check(LIB.cct_graph_create(arr, len(descs), ctypes.byref(h)))
+        else:
+            h = _handle
         self.handle = h
         self.descs = list(descs)
         self.shapes = [output_shape(d) for d in descs]
@@ -264,6 +312,20 @@ class Graph:
     def reset(self):
         check(LIB.cct_graph_reset(self.handle))
         return 0
+
+    def save(self):
+        """Checkpoint record (numpy uint32 words): layer descriptors, constant
+        filters and the step count."""
+        return _save_record(LIB.cct_graph_save, self.handle)
+
+    @classmethod
+    def restore(cls, words):
+        import numpy as np
+        w = np.ascontiguousarray(words, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        check(LIB.cct_graph_restore(ctypes.c_void_p(w.ctypes.data), w.size, ctypes.byref(h)))
+        _, descs, _ = describe_record(w)
+        return cls(descs, _handle=h)
 
     def close(self):
         if self.handle:

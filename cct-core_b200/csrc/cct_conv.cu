@@ -222,6 +222,26 @@ struct cct_conv_plan {
   float *d_x, *d_f, *d_y;
 };
 
+namespace cct {
+
+int plan_record_parts(const cct_conv_plan *p, cct_conv_desc *desc, const float **dev_filter, size_t *elems,
+                      int *device) {
+  if (!p) return set_error(CCT_EINVAL, "null plan");
+  *desc = p->desc;
+  *dev_filter = p->static_filter;
+  *elems = p->f_elems;
+  *device = p->device;
+  return CCT_OK;
+}
+
+int plan_filter_elems(const cct_conv_plan *p, size_t *elems) {
+  if (!p) return set_error(CCT_EINVAL, "null plan");
+  *elems = p->f_elems;
+  return CCT_OK;
+}
+
+}  // namespace cct
+
 extern "C" {
 
 void cct_conv_desc_init(cct_conv_desc *d) {

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "cct_conv.h"
 
@@ -108,6 +109,22 @@ int launch_fa_f32(const ConvGeom &g, const float *x, const float *f, float *y, f
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);
+// Checkpoint records (record.cu): one layer = a descriptor and, for a
+// constant filter, its values.
+struct RecordLayer {
+  cct_conv_desc desc;
+  std::vector<float> filter;
+};
+int record_encode(int kind, int64_t time, const std::vector<RecordLayer> &layers, std::vector<uint32_t> *out);
+int record_decode(const uint32_t *words, size_t n, int *kind, int64_t *time, std::vector<RecordLayer> *layers);
+int record_store(const std::vector<uint32_t> &words, uint32_t *out, size_t capacity, size_t *n_words);
+int record_plan_layer(const cct_conv_plan *p, RecordLayer *out);
+// Plan internals the records need (cct_conv.cu): the descriptor, the device
+// copy of the constant filter (null if none) with its element count, and the
+// plan's device; the filter element count a plan takes.
+int plan_record_parts(const cct_conv_plan *p, cct_conv_desc *desc, const float **dev_filter, size_t *elems,
+                      int *device);
+int plan_filter_elems(const cct_conv_plan *p, size_t *elems);
 int launch_scalar_matrix(int rows, int cols, const float *x, const float *mats, int L, int size, int border,
                          float *y, cudaStream_t stream);
 int launch_separable(int rows, int cols, int planes, const float *x,

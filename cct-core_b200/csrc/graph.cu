@@ -211,6 +211,51 @@ int cct_graph_step_host(cct_graph *g, const float *host_in, float *host_out, voi
 
 int64_t cct_graph_time(const cct_graph *g) { return g ? g->time : -1; }
 
+int cct_graph_save(const cct_graph *g, uint32_t *words, size_t capacity, size_t *n_words) {
+  if (!g) return cct::set_error(CCT_EINVAL, "null graph");
+  std::vector<cct::RecordLayer> layers(g->plans.size());
+  for (size_t i = 0; i < g->plans.size(); ++i) {
+    int rc = cct::record_plan_layer(g->plans[i], &layers[i]);
+    if (rc) return rc;
+    layers[i].desc = g->desc[i];
+  }
+  std::vector<uint32_t> w;
+  cct::record_encode(2, g->time, layers, &w);
+  return cct::record_store(w, words, capacity, n_words);
+}
+
+int cct_graph_restore(const uint32_t *words, size_t n_words, cct_graph **out) {
+  if (!out) return cct::set_error(CCT_EINVAL, "null graph output");
+  *out = nullptr;
+  int kind = 0;
+  int64_t time = 0;
+  std::vector<cct::RecordLayer> layers;
+  int rc = cct::record_decode(words, n_words, &kind, &time, &layers);
+  if (rc) return rc;
+  if (kind != 2) return cct::set_error(CCT_EINVAL, "the record holds a plan, not a graph");
+  std::vector<cct_conv_desc> descs;
+  for (const cct::RecordLayer &l : layers) descs.push_back(l.desc);
+  cct_graph *g = nullptr;
+  rc = cct_graph_create(descs.data(), (int32_t)descs.size(), &g);
+  if (rc) return rc;
+  for (size_t i = 0; !rc && i < layers.size(); ++i) {
+    if (layers[i].filter.empty()) continue;
+    size_t need = 0;
+    rc = cct::plan_filter_elems(g->plans[i], &need);
+    if (!rc && need != layers[i].filter.size())
+      rc = cct::set_error(CCT_EINVAL, "record layer %zu filter has %zu values, the layer needs %zu", i + 1,
+                          layers[i].filter.size(), need);
+    if (!rc) rc = cct_graph_set_filter(g, (int32_t)i + 1, layers[i].filter.data());
+  }
+  if (rc) {
+    cct_graph_destroy(g);
+    return rc;
+  }
+  g->time = time;
+  *out = g;
+  return CCT_OK;
+}
+
 int cct_graph_reset(cct_graph *g) {
   if (!g) return cct::set_error(CCT_EINVAL, "null graph");
   g->time = 0;

@@ -215,6 +215,37 @@ int cct_color_plan_destroy(cct_color_plan *plan);
 int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *image,
                          const float *filter, float *out, void *stream);
 
+/* ---- checkpoint records ---------------------------------------------------
+ * What ComputeGraph.write / readFromFile
+ * (src/main/scala/cogx/runtime/ComputeGraph.scala:523-727) save for a kernel
+ * of this backend, in place of the OpenCL kernel's source code and
+ * work-group parameters (platform/opencl/OpenCLDeviceKernel.scala:219-229,
+ * OpenCLRestoredDeviceKernel.scala:53-64).  A plan or graph is determined by
+ * its descriptors and constant filters, so a record holds those (and a
+ * graph's step count); restoring creates new plans on the current device.
+ *
+ * A record is an array of 32-bit words (store it with the saver's
+ * writeIntArray): magic 0x4B544343, format version 1, kind (1 plan,
+ * 2 graph), layer count, step count (low, high word); per layer the number
+ * of descriptor fields (15), the fields image_rows .. flags in declaration
+ * order, the constant filter's element count (low, high; 0 = none) and its
+ * values as IEEE-754 bits; last an FNV-1a 32-bit hash of the preceding
+ * words' bytes (each word little-endian).
+ *
+ * *_save: with words == NULL, only *n_words is set (the size to allocate);
+ * else the record is written if capacity (in words) suffices, CCT_EINVAL
+ * otherwise.  A saved plan's constant filter is read back from the device.
+ * *_restore: CCT_EINVAL on a bad magic, version, kind, length or checksum.
+ * cct_record_describe: the kind, layer count, step count and up to
+ * max_descs layer descriptors of a record, without touching a device. */
+int cct_conv_plan_save(const cct_conv_plan *plan, uint32_t *words,
+                       size_t capacity, size_t *n_words);
+int cct_conv_plan_restore(const uint32_t *words, size_t n_words,
+                          cct_conv_plan **plan);
+int cct_record_describe(const uint32_t *words, size_t n_words, int32_t *kind,
+                        int32_t *n_layers, int64_t *time,
+                        cct_conv_desc *descs, int32_t max_descs);
+
 /* ---- stacked convolution graphs (ComputeGraph step) --------------------- */
 /* A ComputeGraph whose fields form a chain of convolutions: layer i reads
  * layer i-1's output field.  Replaces the reference's ComputeGraph
@@ -247,6 +278,12 @@ int cct_graph_step(cct_graph *graph, int64_t count, void *stream);
 int cct_graph_step_host(cct_graph *graph, const float *host_in, float *host_out, void *stream);
 int64_t cct_graph_time(const cct_graph *graph);
 int cct_graph_reset(cct_graph *graph);
+/* Checkpoint records of a graph (format above): every layer's descriptor and
+ * constant filter, and the step count.  Restoring recreates the graph on the
+ * current device with zeroed fields and the saved step count. */
+int cct_graph_save(const cct_graph *graph, uint32_t *words, size_t capacity,
+                   size_t *n_words);
+int cct_graph_restore(const uint32_t *words, size_t n_words, cct_graph **graph);
 
 /* ---- request serving (continuous batching) ------------------------------ */
 /* No counterpart in the reference, whose ComputeGraphs are stepped by one

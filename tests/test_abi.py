@@ -175,3 +175,73 @@ def test_color_plan_descriptor_checks():
         pytest.skip("a GPU is present")
     d = _lib.new_desc(image_rows=8, image_cols=8, filter_rows=3, filter_cols=3)
     assert _lib.LIB.cct_color_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.ENODEV
+
+
+def _fnv1a(words):
+    h = 2166136261
+    for w in words:
+        for b in range(4):
+            h ^= (int(w) >> (8 * b)) & 0xFF
+            h = (h * 16777619) & 0xFFFFFFFF
+    return h
+
+
+def _record(kind, layers, time=0):
+    """A checkpoint record built here from the documented word layout."""
+    w = [0x4B544343, 1, kind, len(layers), time & 0xFFFFFFFF, time >> 32]
+    for fields, filt in layers:
+        w += [15] + [int(v) & 0xFFFFFFFF for v in fields]
+        n = len(filt)
+        w += [n & 0xFFFFFFFF, n >> 32]
+        w += list(np.asarray(filt, dtype=np.float32).view(np.uint32))
+    w.append(_fnv1a(w))
+    return np.array(w, dtype=np.uint32)
+
+
+def test_checkpoint_record_format_and_checks():
+    """cct_record_describe parses the documented layout (no device) and
+    rejects bad magic, versions, checksums and lengths."""
+    fields = [64, 64, 512, 5, 5, 2048, 16, _lib.BORDER_ZERO, _lib.CROSS_CORRELATION, _lib.SAMPLE_NONE, 1,
+              _lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, _lib.PREC_BF16X3, 0, 1]
+    filt = np.linspace(-1, 1, 2048 * 25, dtype=np.float32)
+    rec = _record(1, [(fields, filt)])
+    kind, descs, t = _lib.describe_record(rec)
+    assert kind == 1 and t == 0 and len(descs) == 1
+    d = descs[0]
+    assert (d.image_rows, d.image_cols, d.image_planes, d.filter_planes, d.batch_size) == (64, 64, 512, 2048, 16)
+    assert (d.vector_mode, d.precision, d.flags) == (_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, _lib.PREC_BF16X3, 1)
+    assert d.struct_size == ctypes.sizeof(_lib.ConvDesc)
+    g = _record(2, [(fields, []), (fields, filt[:10])], time=(5 << 32) + 7)
+    kind, descs, t = _lib.describe_record(g)
+    assert kind == 2 and len(descs) == 2 and t == (5 << 32) + 7
+    for bad, msg in [(np.concatenate([[0x12345678], rec[1:]]), "magic"),
+                     (rec[:-2], "checksum"),
+                     (np.concatenate([rec[:-1], [rec[-1] ^ 1]]), "checksum"),
+                     (rec[:5], "too short")]:
+        with pytest.raises(_lib.CctError, match=msg):
+            _lib.describe_record(bad)
+    v2 = rec.copy()
+    v2[1] = 2
+    v2[-1] = _fnv1a(v2[:-1])
+    with pytest.raises(_lib.CctError, match="version 2"):
+        _lib.describe_record(v2)
+    short = _record(1, [(fields, filt)])[:-1]
+    short = np.concatenate([short[:-100], [_fnv1a(short[:-100])]]).astype(np.uint32)
+    with pytest.raises(_lib.CctError, match="truncated"):
+        _lib.describe_record(short)
+
+
+def test_checkpoint_restore_needs_a_device_and_save_a_plan():
+    import torch
+    h = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    assert _lib.LIB.cct_conv_plan_save(None, None, 0, ctypes.byref(n)) == _lib.EINVAL
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    fields = [16, 16, 0, 3, 3, 0, 1, 0, 1, 0, 1, 0, 0, 0, 0]
+    rec = _record(1, [(fields, np.ones(9, np.float32))])
+    assert _lib.LIB.cct_conv_plan_restore(ctypes.c_void_p(rec.ctypes.data), rec.size, ctypes.byref(h)) == _lib.ENODEV
+    grec = _record(2, [(fields, [])])
+    assert _lib.LIB.cct_conv_plan_restore(ctypes.c_void_p(grec.ctypes.data), grec.size,
+                                          ctypes.byref(h)) == _lib.EINVAL
+    assert "graph, not a plan" in _lib.LIB.cct_last_error_string().decode()

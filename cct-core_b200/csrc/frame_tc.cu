@@ -110,6 +110,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = bars.tmem_slot;
+  // The set-up above touches no global memory, so it may overlap the previous
+  // kernel in the stream (launched with programmatic serialisation): the
+  // image, the packed filters and the output are only touched after this.
+  grid_dependency_wait();
+  allow_dependent_launch();
 
   const int RS = g.R * g.S;
   const int npix = g.OH * g.OW;
@@ -376,6 +381,10 @@ __global__ void pack_filters_kernel(ConvGeom g, const float *__restrict__ f, uin
   // (launch_pack_filters checks); 64-bit division would dominate this kernel
   const int RS = g.R * g.S;
   const int total = nblocks * NCB * RS * NT * CB;
+  // the previous kernel (the last launch that read the packed operand) must
+  // be done before it is rewritten; the consuming kernel may be scheduled now
+  grid_dependency_wait();
+  allow_dependent_launch();
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
     const int ci = idx % CB;
     int rest = idx / CB;
@@ -432,7 +441,18 @@ int launch_cb(const TcParams &p0, const float *x, cudaStream_t st) {
       have = smem;
     }
   }
-  kern<<<p.grid, kThreads, smem, st>>>(map, p);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = dim3(p.grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  rc = check_cuda(cudaLaunchKernelEx(&cfg, kern, map, p), "frame_tc_kernel launch");
+  if (rc) return rc;
   count_launches(1);
   return check_cuda(cudaGetLastError(), "frame_tc_kernel launch");
 }
@@ -495,7 +515,18 @@ int launch_pack_filters(const TcParams &p, const float *f, uint8_t *packed, cuda
   const long long total = (long long)p.nblocks * p.NCB * p.g.R * p.g.S * p.NT * p.CB;
   if (total > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "packed filter operand too large");
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  pack_filters_kernel<<<blocks, 256, 0, st>>>(p.g, f, packed, p.NT, p.CB, p.NCB, p.nblocks);
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(256);
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int rc = check_cuda(cudaLaunchKernelEx(&cfg, pack_filters_kernel, p.g, f, packed, p.NT, p.CB, p.NCB, p.nblocks),
+                      "pack_filters_kernel launch");
+  if (rc) return rc;
   count_launches(1);
   return check_cuda(cudaGetLastError(), "pack_filters_kernel launch");
 }

@@ -127,6 +127,19 @@ int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols,
 
 namespace cct {
 
+// ---- programmatic dependent launch ----------------------------------------
+// A kernel launched with programmatic stream serialisation may start while
+// the previous kernel in the stream is still running.  Everything before
+// grid_dependency_wait() must not read what earlier work writes nor write
+// what it reads; the wait returns once the previous grid has completed and
+// its memory is visible (at once for a normal launch).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+// Lets the next kernel in the stream be scheduled now (it still waits for
+// this grid's completion at its own grid_dependency_wait()).
+__device__ __forceinline__ void allow_dependent_launch() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // ---- tcgen05 (5th-generation tensor core, tensor memory) ------------------
 
 // One lane of the (fully converged) warp returns true.

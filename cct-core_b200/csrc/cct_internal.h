@@ -109,6 +109,26 @@ int launch_fa_f32(const ConvGeom &g, const float *x, const float *f, float *y, f
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);
+// Launch with programmatic stream serialisation: the kernel may be scheduled
+// while the previous kernel in the stream runs, and must call
+// grid_dependency_wait() (sm100_util.cuh) before it touches global memory
+// that earlier work reads or writes.
+template <typename... Params, typename... Args>
+int launch_pdl(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+               const char *what, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return check_cuda(cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...), what);
+}
+
 // Checkpoint records (record.cu): one layer = a descriptor and, for a
 // constant filter, its values.
 struct RecordLayer {

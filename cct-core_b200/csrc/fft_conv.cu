@@ -31,6 +31,7 @@
 
 #include "cct_internal.h"
 #include "fft_conv.h"
+#include "sm100_util.cuh"
 #include "tile_common.cuh"
 
 namespace cct {
@@ -231,6 +232,8 @@ template <int SRC, int LOGN>
 __global__ void __launch_bounds__(kRowThreads, 4)
     fft_rows_r2c(FftParams p, const float *__restrict__ src, float2 *__restrict__ spec, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
+  grid_dependency_wait();  // launched with programmatic serialisation
+  allow_dependent_launch();
   constexpr int N = 1 << LOGN, T = N / 16, per = kRowThreads / T;
   const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
   const int gr = blockIdx.x * per + sub;
@@ -295,6 +298,8 @@ template <int MODE, int LOGR>
 __global__ void __launch_bounds__(kColThreads, 2)
     fft_cols(FftParams p, float2 *__restrict__ spec, const float2 *__restrict__ G, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
+  grid_dependency_wait();  // launched with programmatic serialisation
+  allow_dependent_launch();
   constexpr int Fr = 1 << LOGR, T = Fr / 16, CW = kColThreads / T;
   const int ncol = p.Fc / 2 + 1;
   const int cblocks = (ncol + CW - 1) / CW;
@@ -340,6 +345,8 @@ template <int LOGN>
 __global__ void __launch_bounds__(kRowThreads, 4)
     fft_rows_c2r(FftParams p, const float2 *__restrict__ spec, float *__restrict__ y, int planes) {
   extern __shared__ __align__(16) float2 fsm[];
+  grid_dependency_wait();  // launched with programmatic serialisation
+  allow_dependent_launch();
   const ConvGeom &g = p.g;
   constexpr int N = 1 << LOGN, T = N / 16, per = kRowThreads / T;
   const int sub = threadIdx.x / T, tt = threadIdx.x - sub * T;
@@ -541,8 +548,8 @@ int launch_cols_t(const FftParams &p, float2 *spec, const float2 *G, int planes,
   int rc = set_smem(fft_cols<MODE, L>, smem);
   if (rc) return rc;
   const int cblocks = (p.Fc / 2 + 1 + cw - 1) / cw;
-  fft_cols<MODE, L><<<cblocks * planes, kColThreads, smem, st>>>(p, spec, G, planes);
-  return CCT_OK;
+  return launch_pdl(fft_cols<MODE, L>, dim3(cblocks * planes), dim3(kColThreads), smem, st, "fft_cols launch", p,
+                    spec, G, planes);
 }
 
 template <int MODE>
@@ -566,8 +573,8 @@ int launch_r2c_t(const FftParams &p, const float *src, float2 *spec, int planes,
   row_shape(p, p.Fr * planes, &per, &blocks, &smem);
   int rc = set_smem(fft_rows_r2c<SRC, L>, smem);
   if (rc) return rc;
-  fft_rows_r2c<SRC, L><<<blocks, kRowThreads, smem, st>>>(p, src, spec, planes);
-  return CCT_OK;
+  return launch_pdl(fft_rows_r2c<SRC, L>, dim3(blocks), dim3(kRowThreads), smem, st, "fft_rows_r2c launch", p,
+                    src, spec, planes);
 }
 
 template <int L>
@@ -577,8 +584,8 @@ int launch_c2r_t(const FftParams &p, const float2 *spec, float *y, int planes, c
   row_shape(p, p.g.OH * planes, &per, &blocks, &smem);
   int rc = set_smem(fft_rows_c2r<L>, smem);
   if (rc) return rc;
-  fft_rows_c2r<L><<<blocks, kRowThreads, smem, st>>>(p, spec, y, planes);
-  return CCT_OK;
+  return launch_pdl(fft_rows_c2r<L>, dim3(blocks), dim3(kRowThreads), smem, st, "fft_rows_c2r launch", p, spec,
+                    y, planes);
 }
 
 int launch_fft_filter_spectrum(const FftParams &p, const float *f, float2 *G, cudaStream_t st) {

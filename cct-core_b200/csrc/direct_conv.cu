@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "cct_internal.h"
+#include "sm100_util.cuh"
 #include "tile_common.cuh"
 
 namespace cct {
@@ -25,6 +26,7 @@ __global__ void __launch_bounds__(kThreads)
     direct_fixed_kernel(ConvGeom g, const float *__restrict__ x,
                         const float *__restrict__ f, float *__restrict__ y,
                         int tiles_x, int tiles_y) {
+  grid_dependency_wait();  // launched with programmatic serialisation: nothing global before this
   constexpr int TW = kTX * U, TH = kTY * V;
   constexpr int IN_COLS = (TW - 1) * DOWN + S;
   constexpr int IN_ROWS = (TH - 1) * DOWN + R;
@@ -130,6 +132,7 @@ __global__ void __launch_bounds__(kThreads)
                           const float *__restrict__ f, float *__restrict__ y,
                           int tiles_x, int tiles_y, int in_rows, int in_cols,
                           int pitch) {
+  grid_dependency_wait();  // launched with programmatic serialisation: nothing global before this
   extern __shared__ __align__(16) float smem[];
   float *tile = smem;
   float *wf = smem + in_rows * pitch;
@@ -210,10 +213,10 @@ int launch_fixed(const ConvGeom &g, const float *x, const float *f, float *y,
   const int tiles_x = (g.OW + TW - 1) / TW, tiles_y = (g.OH + TH - 1) / TH;
   const long long blocks = (long long)tiles_x * tiles_y * g.pout;
   if (blocks > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "direct convolution grid too large");
-  direct_fixed_kernel<R, S, DOWN, U, V>
-      <<<(unsigned)blocks, kThreads, 0, st>>>(g, x, f, y, tiles_x, tiles_y);
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "direct_fixed_kernel launch");
+  const int rc = launch_pdl(direct_fixed_kernel<R, S, DOWN, U, V>, dim3((unsigned)blocks), dim3(kThreads), 0, st,
+                            "direct_fixed_kernel launch", g, x, f, y, tiles_x, tiles_y);
+  if (!rc) count_launches(1);
+  return rc;
 }
 
 int launch_generic(const ConvGeom &g, const float *x, const float *f, float *y,
@@ -237,10 +240,10 @@ int launch_generic(const ConvGeom &g, const float *x, const float *f, float *y,
   }
   const long long blocks = (long long)tiles_x * tiles_y * g.pout;
   if (blocks > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "direct convolution grid too large");
-  direct_generic_kernel<<<(unsigned)blocks, kThreads, smem, st>>>(g, x, f, y, tiles_x, tiles_y,
-                                                                  in_rows, in_cols, pitch);
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "direct_generic_kernel launch");
+  const int rc = launch_pdl(direct_generic_kernel, dim3((unsigned)blocks), dim3(kThreads), smem, st,
+                            "direct_generic_kernel launch", g, x, f, y, tiles_x, tiles_y, in_rows, in_cols, pitch);
+  if (!rc) count_launches(1);
+  return rc;
 }
 
 }  // namespace

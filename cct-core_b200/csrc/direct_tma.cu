@@ -53,6 +53,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm)
     fence_barrier_init();
   }
   __syncthreads();
+  grid_dependency_wait();  // launched with programmatic serialisation: global memory only after this
+  allow_dependent_launch();  // persistent: every CTA is resident already
 
   auto decode = [&](int i, int &o, int &tyi, int &txi) {
     txi = i % tiles_x;
@@ -231,9 +233,10 @@ int launch_tma(const ConvGeom &g, const float *x, const float *f, float *y, cuda
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, T::SMEM);
   const int grid = (int)std::min<long long>(total, (long long)std::max(per_sm, 1) * sms);
-  kern<<<grid, kThreads, T::SMEM, st>>>(map, g, f, y, tiles_x, tiles_y, (int)total, err);
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "direct_tma_kernel launch");
+  const int rc2 = launch_pdl(kern, dim3(grid), dim3(kThreads), T::SMEM, st, "direct_tma_kernel launch", map, g, f,
+                             y, tiles_x, tiles_y, (int)total, err);
+  if (!rc2) count_launches(1);
+  return rc2;
 }
 
 }  // namespace

@@ -12,6 +12,7 @@
 // output matches the reference (per-row fma chain, row sum, plane sum), so
 // results are bit-identical to the FP32 CPU restatement.
 #include "cct_internal.h"
+#include "sm100_util.cuh"
 #include "tile_common.cuh"
 
 namespace cct {
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     frame_f32_kernel(ConvGeom g, const float *__restrict__ x,
                      const float *__restrict__ f, float *__restrict__ y,
                      int tiles_x, int tiles_y, int kblocks) {
+  grid_dependency_wait();  // launched with programmatic serialisation: nothing global before this
   using T = FrameTile<R, S, DOWN>;
   constexpr int E = (kU - 1) * DOWN + S;
   constexpr int E4 = (E + 3) / 4;
@@ -182,10 +184,10 @@ int launch(const ConvGeom &g, const float *x, const float *f, float *y, cudaStre
   if (blocks > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "frame grid too large");
   const size_t smem = 2 * sizeof(float) * T::STAGE;
   static_assert(2 * sizeof(float) * T::STAGE <= 48 * 1024, "frame stages exceed the default smem limit");
-  frame_f32_kernel<R, S, DOWN><<<(unsigned)blocks, kThreads, smem, st>>>(g, x, f, y, tiles_x, tiles_y,
-                                                                        kblocks);
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "frame_f32_kernel launch");
+  const int rc = launch_pdl(frame_f32_kernel<R, S, DOWN>, dim3((unsigned)blocks), dim3(kThreads), smem, st,
+                            "frame_f32_kernel launch", g, x, f, y, tiles_x, tiles_y, kblocks);
+  if (!rc) count_launches(1);
+  return rc;
 }
 
 }  // namespace

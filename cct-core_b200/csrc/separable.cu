@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(kThreads)
     separable_fused_t(int rows, int cols, const float *__restrict__ x, const float *__restrict__ rf,
                       const float *__restrict__ cf, int border, int orient, float *__restrict__ y,
                       int tiles_x, int tiles_y, long long tiles) {
+  grid_dependency_wait();  // launched with programmatic serialisation: nothing global before this
   using T = SepTile<RL, CL>;
   constexpr int IR = T::IR, IC = T::IC, MP = T::MP, U = T::U, hr = T::hr, hc = T::hc, ICU = T::ICU;
   __shared__ float img[IR * IC];
@@ -218,10 +219,10 @@ template <int RL, int CL>
 int launch_fused_t(int rows, int cols, const float *x, const float *rf, const float *cf, int border,
                    int orient, float *y, int tiles_x, int tiles_y, long long tiles, cudaStream_t st) {
   if (tiles > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "separable: grid too large");
-  separable_fused_t<RL, CL><<<(unsigned)tiles, kThreads, 0, st>>>(rows, cols, x, rf, cf, border, orient, y,
-                                                                  tiles_x, tiles_y, tiles);
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "separable launch");
+  const int rc = launch_pdl(separable_fused_t<RL, CL>, dim3((unsigned)tiles), dim3(kThreads), 0, st,
+                            "separable launch", rows, cols, x, rf, cf, border, orient, y, tiles_x, tiles_y, tiles);
+  if (!rc) count_launches(1);
+  return rc;
 }
 
 // BorderZero with TMA staging: persistent CTAs walk 64 x 128 output tiles
@@ -265,6 +266,8 @@ __global__ void __launch_bounds__(kThreads)
     fence_barrier_init();
   }
   __syncthreads();
+  grid_dependency_wait();  // launched with programmatic serialisation: global memory only after this
+  allow_dependent_launch();  // persistent: every CTA is resident already
   auto decode = [&](int i, int &pl, int &tyi, int &txi) {
     txi = i % tiles_x;
     const int q = i / tiles_x;
@@ -398,10 +401,10 @@ int launch_tma_t(int rows, int cols, int planes, const float *x, const float *rf
     ready.fetch_or(1ull << dev);
   }
   const int grid = (int)(total < grid_cap[dev] ? total : grid_cap[dev]);
-  kern<<<grid, kThreads, T::SMEM, st>>>(map, rows, cols, rf, cf, orient, y, tiles_x, tiles_y, (int)total,
-                                        device_error_word());
-  count_launches(1);
-  return check_cuda(cudaGetLastError(), "separable_tma launch");
+  const int rc2 = launch_pdl(kern, dim3(grid), dim3(kThreads), T::SMEM, st, "separable_tma launch", map, rows, cols,
+                             rf, cf, orient, y, tiles_x, tiles_y, (int)total, device_error_word());
+  if (!rc2) count_launches(1);
+  return rc2;
 }
 
 // Row lengths 1..9 (odd) with their x-offset remainder, column lengths 1..9

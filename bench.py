@@ -146,6 +146,34 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- workloads
+def errors_vs(y, ref):
+    """Normwise max and RMS relative error of y against an FP64 reference."""
+    import numpy as np
+    d = np.asarray(y, np.float64) - ref
+    return {"max_rel": float(np.abs(d).max() / np.abs(ref).max()),
+            "rms_rel": float(np.sqrt((d * d).mean() / (ref * ref).mean()))}
+
+
+def np_conv_same(x, f, flip):
+    """FP64 zero-border 'same' filter bank in numpy (the accuracy reference the
+    bench reports against; the tests check against the oracle):
+    y[k, i, j] = sum_{c, r, s} x[c, i + r - h, j + s - h] * f'[k, c, r, s],
+    f' = f flipped in r and s when `flip`."""
+    import numpy as np
+    C, H, W = x.shape
+    K, _, R, S = f.shape
+    h = (R - 1) // 2
+    xp = np.pad(x.astype(np.float64), ((0, 0), (h, h), (h, h)))
+    f = f.astype(np.float64)
+    if flip:
+        f = f[:, :, ::-1, ::-1]
+    y = np.zeros((K, H * W))
+    for r in range(R):
+        for s in range(S):
+            y += f[:, :, r, s] @ xp[:, r:r + H, s:s + W].reshape(C, -1)
+    return y.reshape(K, H, W)
+
+
 def frame_workload(precision):
     """Build the projectFrame/backProjectFrame pair; returns a dict of callables."""
     import torch
@@ -226,6 +254,17 @@ def frame_workload(precision):
     def e2e_finish():  # the timed region closes after both streams drain
         streams[0].wait_stream(streams[1])
 
+    def frame_errors():
+        """Image 0 of one forward and one backward step against FP64 numpy."""
+        step()
+        torch.cuda.synchronize()
+        fn = f.double().cpu().numpy().reshape(K, Cin, R, R)
+        fwd_ref = np_conv_same(xs[0][:Cin].double().cpu().numpy(), fn, flip=False)
+        bwd_ref = np_conv_same(gs[0][:K].double().cpu().numpy(), fn.transpose(1, 0, 2, 3), flip=True)
+        return {"projectFrame": errors_vs(ys[0][:K].cpu().numpy(), fwd_ref),
+                "backProjectFrame": errors_vs(dxs[0][:Cin].cpu().numpy(), bwd_ref),
+                "sample": "image 0 of the batch"}
+
     nbytes = lambda t: t.numel() * 4  # noqa: E731
     return {
         "step": step, "e2e_step": e2e_step, "e2e_begin": e2e_begin, "e2e_finish": e2e_finish,
@@ -238,6 +277,7 @@ def frame_workload(precision):
                    "R": R, "border": "BorderZero", "l2": "6 rotating input/output sets (288 MB > 126 MB L2)"},
         "dtype": "f32" if precision == "fp32" else "bf16x3 split, f32 accumulate",
         "keep": (fwd, bwd, xs, gs, ys, dxs, f, hx, hg, hf, hy, hdx),
+        "extra": {"error_vs_fp64": frame_errors()},
         "kernel": "frame_f32_kernel" if precision == "fp32" else "frame_tc_kernel",
         "bytes_per_launch": 4 * (B * Cin * H * W + K * Cin * R * R + B * K * H * W),
     }
@@ -287,7 +327,11 @@ def plain_workload():
                                                y.data_ptr(), ctypes.c_void_p(stream)))
     sep_s = time_single_launch(separable, reps=10)
     sep_bytes = 2 * 4 * P * H * W
-    extra = {"single_plane_256x256_us": round(single_s * 1e6, 2),
+    step()
+    torch.cuda.synchronize()
+    ref = np_conv_same(x[:1].double().cpu().numpy(), f.double().cpu().numpy()[None, None], flip=True)
+    extra = {"error_vs_fp64": dict(errors_vs(y[:1].cpu().numpy(), ref), sample="plane 0"),
+             "single_plane_256x256_us": round(single_s * 1e6, 2),
              "separable_5+5_4096x256x256": {"ms": round(sep_s * 1e3, 4),
                                             "GB/s": round(sep_bytes / sep_s / 1e9, 1)}}
 

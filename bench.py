@@ -461,6 +461,7 @@ def graph_workload(precision):
             fs.append((rng.standard_normal((kc, r, s_)) * np.sqrt(2.0 / (c * r * s_))).astype(np.float32))
         st.set_filters(fs)
         st.input.uniform_(-1, 1)
+        st.bench_filters = fs
         return st
 
     B = 64
@@ -490,6 +491,33 @@ def graph_workload(precision):
         for b in (1, 8, 64):
             extra["by_batch"][f"{p_name}_b{b}"] = side(b, p)
 
+    def graph_errors():
+        """Image 0 of a batch-64 step against FP64 numpy (same-size zero-border
+        layers, then the step-2 subsample, ReLU between layers): through all
+        eight layers from the input (errors compound), and per layer from the
+        GPU's own input to that layer."""
+        stack.step(1, stream)
+        torch.cuda.synchronize()
+        widths = [64, 64, 128, 128, 256, 256, 512, 512]
+
+        def layer(i, a):
+            a = np_conv_same(a, stack.bench_filters[i].reshape(widths[i], a.shape[0], 3, 3), flip=False)
+            if i in (1, 3, 5):
+                a = a[:, ::2, ::2]
+            return np.maximum(a, 0.0) if i < 7 else a
+
+        a = stack.input[:3].double().cpu().numpy()
+        per_layer = []
+        for i in range(8):
+            gin = stack.field(i)[:a.shape[0] if i == 0 else widths[i - 1]].double().cpu().numpy()
+            gout = stack.field(i + 1)[:widths[i]].cpu().numpy()
+            per_layer.append(errors_vs(gout, layer(i, gin))["max_rel"])
+            a = layer(i, a)
+        out = stack.field(len(stack.descs))[:512].cpu().numpy()
+        return dict(errors_vs(out, a), per_layer_max_rel=per_layer,
+                    sample="image 0; all eight layers from the input, and each layer from its GPU input")
+
+    extra["error_vs_fp64"] = graph_errors()
     hx = stack.input.cpu().pin_memory()
     hy = torch.empty(stack.field_shapes[-1]).pin_memory()
 

@@ -247,16 +247,25 @@ __global__ void __launch_bounds__(kRowThreads, 4)
     if (active) plane_pair(g, pl, 0, &ip, &fp);
     const float *xp = src + (size_t)ip * g.H * g.W;
     const int sr = active ? expand_index(row, g.H, p.Fr, g.border) : -1;
+    // positions inside the field map to themselves: one 8-byte load per pair
+    // (an 8-byte aligned plane of even width keeps every row aligned); the
+    // border positions take the expansion rule
+    const bool pairs = sr >= 0 && (g.W & 1) == 0 && (reinterpret_cast<uintptr_t>(xp) & 7) == 0;
+    const float2 *row2 = reinterpret_cast<const float2 *>(xp + (size_t)(sr < 0 ? 0 : sr) * g.W);
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
       const int n = tt + m * T;
-      float e[2];
+      if (pairs && 2 * n + 1 < g.W) {
+        v[m] = __ldg(row2 + n);
+      } else {
+        float e[2];
 #pragma unroll
-      for (int k = 0; k < 2; ++k) {
-        const int sc = expand_index(2 * n + k, g.W, p.Fc, g.border);
-        e[k] = (sr >= 0 && sc >= 0) ? __ldg(xp + (size_t)sr * g.W + sc) : 0.0f;
+        for (int k = 0; k < 2; ++k) {
+          const int sc = expand_index(2 * n + k, g.W, p.Fc, g.border);
+          e[k] = (sr >= 0 && sc >= 0) ? __ldg(xp + (size_t)sr * g.W + sc) : 0.0f;
+        }
+        v[m] = make_float2(e[0], e[1]);
       }
-      v[m] = make_float2(e[0], e[1]);
     }
   } else {
     const float *fp = src + (size_t)pl * g.R * g.S;
@@ -374,10 +383,21 @@ __global__ void __launch_bounds__(kRowThreads, 4)
   if (!active) return;
   float *yr = y + ((size_t)pl * g.OH + row) * g.OW;
   const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
-  for (int j = tt; j < g.OW; j += T) {
-    const float2 z = s[pad16(j >> 1)];
-    const float o = (j & 1) ? z.y : z.x;
-    yr[j] = relu ? fmaxf(o, 0.0f) : o;
+  if ((g.OW & 1) == 0 && (reinterpret_cast<uintptr_t>(y) & 7) == 0) {
+    // an aligned field of even width keeps every output row 8-byte aligned:
+    // one pair per store
+    float2 *yr2 = reinterpret_cast<float2 *>(yr);
+    for (int j = tt; j < g.OW / 2; j += T) {
+      float2 z = s[pad16(j)];
+      if (relu) z = make_float2(fmaxf(z.x, 0.0f), fmaxf(z.y, 0.0f));
+      yr2[j] = z;
+    }
+  } else {
+    for (int j = tt; j < g.OW; j += T) {
+      const float2 z = s[pad16(j >> 1)];
+      const float o = (j & 1) ? z.y : z.x;
+      yr[j] = relu ? fmaxf(o, 0.0f) : o;
+    }
   }
 }
 

@@ -50,6 +50,14 @@ __device__ __forceinline__ float2 conjf2(float2 a) { return make_float2(a.x, -a.
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
 __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
+// Spectrum layout of one plane (Fr rows x ld columns, ld a multiple of 4):
+// blocks of 4 columns, each block all Fr rows of its 4 columns (32 bytes per
+// row).  A row pass reads and writes 32-byte row segments; a column pass
+// reads its columns as one contiguous stretch per block.
+__host__ __device__ __forceinline__ size_t spec_index(int r, int c, int Fr) {
+  return ((size_t)(c >> 2) * Fr + r) * 4 + (c & 3);
+}
+
 // multiply by -i (forward transform) or +i (inverse)
 template <bool INV>
 __device__ __forceinline__ float2 rot(float2 a) {
@@ -289,13 +297,13 @@ __global__ void __launch_bounds__(kRowThreads, 4)
   if (!active) return;
   // X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i,
   // W = exp(-2 pi i / Fc), k = 0..N
-  float2 *out = spec + ((size_t)pl * p.Fr + row) * p.ld;
+  float2 *out = spec + (size_t)pl * p.Fr * p.ld;
   for (int k = tt; k <= N; k += T) {
     const float2 zk = s[pad16(k == N ? 0 : k)], zn = conjf2(s[pad16(k == 0 ? 0 : N - k)]);
     const float2 e = make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y + zn.y));
     const float2 dd = make_float2(0.5f * (zk.x - zn.x), 0.5f * (zk.y - zn.y));
     const float2 o = make_float2(dd.y, -dd.x);  // dd / i
-    out[k] = cadd(e, cmul(__ldg(p.tw_2n + k), o));
+    out[spec_index(row, k, p.Fr)] = cadd(e, cmul(__ldg(p.tw_2n + k), o));
   }
 }
 
@@ -318,33 +326,33 @@ __global__ void __launch_bounds__(kColThreads, 2)
   // column stride = 8 (mod 16) complex: the CW columns a warp touches fall
   // on alternate halves of the banks
   float2 *s = fsm + c * col_stride(Fr);
-  float2 *sp = spec + (size_t)pl * Fr * p.ld + col;
+  float2 *sp = spec + (size_t)pl * Fr * p.ld + spec_index(0, col, Fr);  // row r at sp[4 r]
   float2 v[16];
 #pragma unroll
-  for (int m = 0; m < 16; ++m) v[m] = active ? sp[(size_t)(tt + m * T) * p.ld] : make_float2(0.0f, 0.0f);
+  for (int m = 0; m < 16; ++m) v[m] = active ? sp[(size_t)(tt + m * T) * 4] : make_float2(0.0f, 0.0f);
   fft_passes<LOGR, false>(s, v, tt, p.tw_r);
   if (MODE == 0) {
     int ip, fp;
     plane_pair(p.g, pl, 0, &ip, &fp);
-    const float2 *gp = G + (size_t)fp * Fr * p.ld + col;
+    const float2 *gp = G + (size_t)fp * Fr * p.ld + spec_index(0, col, Fr);
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
       const int r = tt + m * T;
-      v[m] = active ? cmul(s[pad16(r)], __ldg(gp + (size_t)r * p.ld)) : make_float2(0.0f, 0.0f);
+      v[m] = active ? cmul(s[pad16(r)], __ldg(gp + (size_t)r * 4)) : make_float2(0.0f, 0.0f);
     }
     fft_passes<LOGR, true>(s, v, tt, p.tw_r);
     if (!active) return;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
       const int r = tt + m * T;
-      sp[(size_t)r * p.ld] = s[pad16(r)];
+      sp[(size_t)r * 4] = s[pad16(r)];
     }
   } else {
     if (!active) return;
 #pragma unroll
     for (int m = 0; m < 16; ++m) {
       const int r = tt + m * T;
-      sp[(size_t)r * p.ld] = cscale(s[pad16(r)], p.scale);
+      sp[(size_t)r * 4] = cscale(s[pad16(r)], p.scale);
     }
   }
 }
@@ -363,7 +371,7 @@ __global__ void __launch_bounds__(kRowThreads, 4)
   const bool active = gr < planes * g.OH;
   const int row = gr % g.OH, pl = gr / g.OH;
   float2 *s = fsm + sub * (N + N / 16);
-  const float2 *in = spec + ((size_t)pl * p.Fr + row) * p.ld;
+  const float2 *in = spec + (size_t)pl * p.Fr * p.ld;
   // Z[k] = E[k] + i O[k], E = (X[k] + conj X[N-k]) / 2, O = (X[k] - conj X[N-k]) / 2 * conj(W^k)
   float2 v[16];
 #pragma unroll
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(kRowThreads, 4)
     const int k = tt + m * T;
     float2 z = make_float2(0.0f, 0.0f);
     if (active) {
-      const float2 xk = __ldg(in + k), xn = conjf2(__ldg(in + N - k));
+      const float2 xk = __ldg(in + spec_index(row, k, p.Fr)), xn = conjf2(__ldg(in + spec_index(row, N - k, p.Fr)));
       const float2 e = make_float2(0.5f * (xk.x + xn.x), 0.5f * (xk.y + xn.y));
       const float2 dd = make_float2(0.5f * (xk.x - xn.x), 0.5f * (xk.y - xn.y));
       const float2 o = cmul(dd, conjf2(__ldg(p.tw_2n + k)));
@@ -476,7 +484,7 @@ bool fft_plan(const ConvGeom &g, FftParams *out) {
     return false;
   p.logN = ilog2(p.Fc / 2);
   p.logR = ilog2(p.Fr);
-  p.ld = ((p.Fc / 2 + 1) + 3) & ~3;  // 32-byte aligned spectrum rows
+  p.ld = ((p.Fc / 2 + 1) + 3) & ~3;  // whole 4-column blocks (spec_index)
   p.scale = 1.0f / ((float)p.Fr * (float)(p.Fc / 2));
   p.spec_elems = (size_t)g.pout * p.Fr * p.ld;
   p.filter_elems = (size_t)g.pf * p.Fr * p.ld;
@@ -540,8 +548,8 @@ void fft_static_spectrum(const FftParams &p, const float *host_filter, std::vect
     for (int r = 0; r < Fr; ++r)
       for (int c = 0; c <= Fc / 2; ++c) {
         const std::complex<double> v = grid[(size_t)r * Fc + c] * scale;
-        o[2 * ((size_t)r * ld + c)] = (float)v.real();
-        o[2 * ((size_t)r * ld + c) + 1] = (float)v.imag();
+        o[2 * spec_index(r, c, Fr)] = (float)v.real();
+        o[2 * spec_index(r, c, Fr) + 1] = (float)v.imag();
       }
   }
 }

@@ -254,6 +254,27 @@ def frame_workload(precision):
     def e2e_finish():  # the timed region closes after both streams drain
         streams[0].wait_stream(streams[1])
 
+    def weight_gradient():
+        """FilterAdjointBlockReduceSum beside the step: the 5x5 filter gradient
+        of the same layer (the image zero-padded to 68x68, the 64x64 output
+        gradient as the 'filter'), FP32 and split BF16, with the BF16 error
+        against the FP32 kernel's result in FP64."""
+        out = {}
+        xa = torch.randn((B * Cin, H + R - 1, W + R - 1), device="cuda", generator=gen)
+        ga = torch.randn((B * K, H, W), device="cuda", generator=gen)
+        ys_ = {}
+        for name, pr in (("fp32", _lib.PREC_FP32), ("bf16x3", _lib.PREC_BF16X3)):
+            pl = _lib.Plan(C.make_desc((H + R - 1, W + R - 1, B * Cin), (H, W, B * K), C.BorderValid,
+                                       _lib.CROSS_CORRELATION, C.NoSamplingConvolution,
+                                       _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM, B, pr))
+            yo = torch.empty((K * Cin, R, R), device="cuda")
+            t = time_single_launch(lambda: pl.run(xa.data_ptr(), ga.data_ptr(), yo.data_ptr(), stream), reps=10)
+            out[name] = {"ms": round(t * 1e3, 4), "GFLOP/s": round(GFLOP_FRAME / t, 1), "plan_algo": pl.algo}
+            ys_[name] = yo.double().cpu().numpy()
+            pl.close()
+        out["bf16x3_vs_fp32"] = errors_vs(ys_["bf16x3"], ys_["fp32"])
+        return out
+
     def frame_errors():
         """Image 0 of one forward and one backward step against FP64 numpy."""
         step()
@@ -277,7 +298,7 @@ def frame_workload(precision):
                    "R": R, "border": "BorderZero", "l2": "6 rotating input/output sets (288 MB > 126 MB L2)"},
         "dtype": "f32" if precision == "fp32" else "bf16x3 split, f32 accumulate",
         "keep": (fwd, bwd, xs, gs, ys, dxs, f, hx, hg, hf, hy, hdx),
-        "extra": {"error_vs_fp64": frame_errors()},
+        "extra": {"error_vs_fp64": frame_errors(), "weight_gradient_5x5": weight_gradient()},
         "kernel": "frame_f32_kernel" if precision == "fp32" else "frame_tc_kernel",
         "bytes_per_launch": 4 * (B * Cin * H * W + K * Cin * R * R + B * K * H * W),
     }

@@ -294,12 +294,13 @@ def convolveFilterAdjoint(field, filter, borderPolicy, samplingPolicy=NoSampling
 
 
 def filterAdjointBlockReduceSum(field, filter, borderPolicy, samplingPolicy=NoSamplingConvolution,
-                                batchSize=1, orientation=_lib.CROSS_CORRELATION):
+                                batchSize=1, orientation=_lib.CROSS_CORRELATION, precision=_lib.PREC_FP32):
     """blockReduceSum(crossCorrelateFilterAdjoint(...), batchSize) fused, the
     form the reference's optimizer emits (FilterAdjointBlockReduceSum): plane
-    w sums the batchSize images' planes in order."""
+    w sums the batchSize images' planes in order.  precision PREC_BF16X3 runs
+    it on the tensor cores (split BF16, within 1e-5 of FP64)."""
     return _run(field, filter, borderPolicy, orientation, samplingPolicy,
-                _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM, batchSize)
+                _lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM, batchSize, precision)
 
 
 def _separable(field, rowFilter, columnFilter, borderPolicy, orientation):

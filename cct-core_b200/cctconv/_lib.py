@@ -22,7 +22,7 @@ SAMPLE_NONE, SAMPLE_DOWN, SAMPLE_UP = 0, 1, 2
 PREC_FP32, PREC_BF16X3 = 0, 1
 ALGO_AUTO, ALGO_DIRECT, ALGO_FFT = 0, 1, 2
 FLAG_RELU = 0x1
-PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT, PLAN_FILTER_ADJOINT = 0, 1, 2, 3, 4
+PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT, PLAN_FILTER_ADJOINT, PLAN_FILTER_ADJOINT_BF16X3 = range(6)
 
 
 class ConvDesc(ctypes.Structure):

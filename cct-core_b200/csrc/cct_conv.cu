@@ -199,7 +199,8 @@ int resolve_geom(const cct_conv_desc *desc, ConvGeom *g) { return resolve(desc, 
 
 using namespace cct;
 
-enum { ALGO_DIRECT = 0, ALGO_FRAME_F32 = 1, ALGO_FRAME_BF16X3 = 2, ALGO_FFT = 3, ALGO_FILTER_ADJOINT = 4 };
+enum { ALGO_DIRECT = 0, ALGO_FRAME_F32 = 1, ALGO_FRAME_BF16X3 = 2, ALGO_FFT = 3, ALGO_FILTER_ADJOINT = 4,
+       ALGO_FILTER_ADJOINT_BF16X3 = 5 };
 
 struct cct_conv_plan {
   cct_conv_desc desc;
@@ -316,10 +317,13 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   TcParams tc{};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (d->precision == CCT_PREC_BF16X3 && !reduce)
-    return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum frame modes only");
+  const bool fa_reduce = g.mode == CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM;
+  if (d->precision == CCT_PREC_BF16X3 && !reduce && !fa_reduce)
+    return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum modes only");
   if (use_fft)
     algo = ALGO_FFT;
+  else if (d->precision == CCT_PREC_BF16X3 && fa_reduce && fa_tc_supported(g))
+    algo = ALGO_FILTER_ADJOINT_BF16X3;
   else if (fa_f32_supported(g))
     algo = ALGO_FILTER_ADJOINT;
   else if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
@@ -345,6 +349,14 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
     rc = check_cuda(cudaMalloc(&p->packed, tc.pack_bytes), "cudaMalloc(packed filters)");
     if (rc) {
       delete p;
+      return rc;
+    }
+  }
+  if (algo == ALGO_FILTER_ADJOINT_BF16X3) {
+    rc = check_cuda(cudaMalloc(&p->fa_work, fa_tc_workspace_bytes(g, sms)),
+                    "cudaMalloc(FilterAdjoint partial sums)");
+    if (rc) {
+      cct_conv_plan_destroy(p);
       return rc;
     }
   }
@@ -446,6 +458,8 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
       return launch_frame_f32(p->g, x, f, y, st);
     case ALGO_FILTER_ADJOINT:
       return launch_fa_f32(p->g, x, f, y, p->fa_work, st);
+    case ALGO_FILTER_ADJOINT_BF16X3:
+      return launch_fa_tc(p->g, x, f, y, p->fa_work, p->err, st);
     case ALGO_FFT: {
       int rc = CCT_OK;
       if (f != p->static_filter || !p->fft_static)

@@ -106,6 +106,12 @@ unsigned *device_error_word();
 bool fa_f32_supported(const ConvGeom &g);
 size_t fa_workspace_bytes(const ConvGeom &g);
 int launch_fa_f32(const ConvGeom &g, const float *x, const float *f, float *y, float *work, cudaStream_t st);
+// FilterAdjointBlockReduceSum on the tensor cores (fa_tc.cu), split BF16:
+// the shapes fa_f32 takes; workspace for the per-split partial sums.
+bool fa_tc_supported(const ConvGeom &g);
+size_t fa_tc_workspace_bytes(const ConvGeom &g, int sms);
+int launch_fa_tc(const ConvGeom &g, const float *x, const float *f, float *y, float *work, unsigned *err,
+                 cudaStream_t st);
 bool frame_f32_supported(const ConvGeom &g);
 int launch_frame_f32(const ConvGeom &g, const float *x, const float *f,
                      float *y, cudaStream_t stream);

@@ -63,9 +63,12 @@ enum { CCT_PLANE_BY_PLANE = 0, CCT_PROJECT_FRAME = 1,
        CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM = 2, CCT_BACK_PROJECT_FRAME = 3,
        CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM = 4, CCT_FILTER_ADJOINT = 5,
        CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM = 6 };
-/* Arithmetic of the multi-plane (frame) kernels.  FP32 is the reference's
+/* Arithmetic of the multi-plane kernels.  FP32 is the reference's
  * arithmetic; BF16X3 splits each FP32 operand into bf16 hi+lo and sums the
- * hi*hi + hi*lo + lo*hi products on tcgen05 tensor cores in FP32. */
+ * hi*hi + hi*lo + lo*hi products on tcgen05 tensor cores in FP32.  BF16X3
+ * applies to the BlockReduceSum modes: the frame modes (PROJECT_FRAME_ and
+ * BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM) and FILTER_ADJOINT_BLOCK_REDUCE_SUM
+ * (the weight gradient, with BorderValid and no sampling). */
 enum { CCT_PREC_FP32 = 0, CCT_PREC_BF16X3 = 1 };
 /* Direct vs FFT (ConvolutionFFTUsePolicy.scala:24-28 UseFFTNever/Always/WhenBest) */
 enum { CCT_ALGO_AUTO = 0, CCT_ALGO_DIRECT = 1, CCT_ALGO_FFT = 2 };
@@ -116,7 +119,8 @@ int cct_conv_plan_create(const cct_conv_desc *desc, cct_conv_plan **plan);
 int cct_conv_plan_destroy(cct_conv_plan *plan);
 
 /* Kernel family the plan chose: 0 direct stencil, 1 frame FP32, 2 frame
- * BF16X3 tensor core, 3 FFT, 4 FilterAdjoint FP32. */
+ * BF16X3 tensor core, 3 FFT, 4 FilterAdjoint FP32, 5 FilterAdjoint BF16X3
+ * tensor core. */
 int cct_conv_plan_algo(const cct_conv_plan *plan, int32_t *algo_out);
 
 /* Static filter (the reference's ConstantFieldKernel filter): its FFT

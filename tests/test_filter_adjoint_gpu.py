@@ -129,3 +129,52 @@ def test_filter_adjoint_weight_gradient_timing():
     got = y.cpu().numpy()
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
     plan.close()
+
+
+TC_CASES = [
+    # C, L, image rows, cols, gradient rows, cols, batch (BorderValid, no sampling)
+    (32, 64, 68, 68, 64, 64, 4),    # the 5x5 weight gradient of a 64x64 layer (M = 800: 7 row tiles)
+    (3, 4, 71, 23, 65, 17, 2),      # gradient width not a multiple of 16, L below 16
+    (5, 72, 20, 21, 16, 17, 3),     # L = 72: two column blocks; 4x5 results
+    (1, 16, 9, 9, 1, 1, 5),         # 1x1 gradient: one pixel per chunk
+    (7, 24, 40, 33, 33, 31, 1),     # one image, 8x3 results
+]
+
+
+@pytest.mark.parametrize("orient", [O.XCORR, O.CONV], ids=["xcorr", "conv"])
+@pytest.mark.parametrize("case", TC_CASES, ids=lambda c: "-".join(map(str, c)))
+def test_filter_adjoint_reduce_tensor_cores(case, orient):
+    """FilterAdjointBlockReduceSum in split BF16 on the tensor cores: normwise
+    max error <= 1e-5 against the FP64 oracle (RMS reported), and the same
+    bits on a second run (the split partial sums are added in split order)."""
+    Cn, L, rows, cols, gr, gc, batch = case
+    rng = np.random.default_rng(rows * 7 + gc)
+    x = rng.standard_normal((batch * Cn, rows, cols)).astype(np.float32)
+    g = rng.standard_normal((batch * L, gr, gc)).astype(np.float32)
+    desc = _lib.new_desc(image_rows=rows, image_cols=cols, image_planes=batch * Cn, filter_rows=gr,
+                         filter_cols=gc, filter_planes=batch * L, batch_size=batch, border=_lib.BORDER_VALID,
+                         orientation=orient, vector_mode=_lib.FILTER_ADJOINT_BLOCK_REDUCE_SUM,
+                         precision=_lib.PREC_BF16X3)
+    plan = _lib.Plan(desc)
+    assert plan.algo == _lib.PLAN_FILTER_ADJOINT_BF16X3
+    plan.close()
+    y1 = _run(desc, x, g)
+    assert _lib.LIB.cct_device_status() == _lib.OK
+    y2 = _run(desc, x, g)
+    od = O.make_desc(rows, cols, gr, gc, planes=batch * Cn, f_planes=batch * L, batch=batch,
+                     border=O.VALID, orient=orient, mode=O.FILTER_ADJOINT_REDUCE)
+    ref = O.conv(od, x, g, np.float64)
+    mx, rms = O.rel_errors(y1.reshape(ref.shape), ref)
+    assert mx <= 1e-5, (mx, rms)
+    assert np.array_equal(y1, y2)
+
+
+def test_filter_adjoint_tensor_cores_through_the_api():
+    rng = np.random.default_rng(3)
+    x = torch.from_numpy(rng.standard_normal((2 * 4, 12, 12)).astype(np.float32)).cuda()
+    g = torch.from_numpy(rng.standard_normal((2 * 8, 10, 10)).astype(np.float32)).cuda()
+    y = C.filterAdjointBlockReduceSum(x, g, C.BorderValid, batchSize=2, precision=_lib.PREC_BF16X3)
+    ref = C.filterAdjointBlockReduceSum(x, g, C.BorderValid, batchSize=2)
+    torch.cuda.synchronize()
+    assert y.shape == ref.shape == (32, 3, 3)
+    assert O.rel_errors(y.cpu().numpy(), ref.cpu().numpy().astype(np.float64))[0] <= 1e-5

@@ -7,7 +7,7 @@
 //
 // GEMM view: D[m][n] = sum_k A[m][k] B[n][k] with rows m = (c, r, s) of the
 // result (M = C*OH*OW), columns n = l (the gradient planes) and the reduction
-// k = (b, i, j) over every image's gradient pixels.  A reduction chunk is 16
+// k = (b, i, j) over every image's gradient pixels.  A reduction chunk is 32
 // consecutive pixels j of one gradient row i of one image b:
 //   A[m][jj] = x[b*C + c](r + i, s + j0 + jj)  (tensor memory, lane m)
 //   B[n][jj] = g'[b*L + l](i, j0 + jj)        (shared memory, K-major)
@@ -38,8 +38,9 @@ namespace {
 constexpr int kFaThreads = 256;
 constexpr int kMT = 128;   // result rows (c, r, s) per tile = TMEM lanes
 constexpr int kNT = 64;    // gradient planes per column block (max)
-constexpr int kKC = 16;    // gradient pixels per reduction chunk
+constexpr int kKC = 32;    // gradient pixels per reduction chunk (two MMA K-steps)
 constexpr int kTmemCols = 256;
+constexpr int kPF = 2;     // chunks whose loads are in flight ahead of the one being built
 
 struct FaTcParams {
   int H, W, Hg, Wg, OH, OW, C, L, B;
@@ -50,25 +51,19 @@ struct FaTcParams {
   unsigned *err;
 };
 
-// Byte offset of (n, k) in one K-major operand image of rows x 16 bf16 (no
-// swizzle): core matrix (8 rows x 8 elements, 128 bytes) at (n/8)*256 + (k/8)*128.
+// Byte offset of (n, k) in one K-major operand image of rows x 32 bf16 (no
+// swizzle): core matrix (8 rows x 8 elements, 128 bytes) at (n/8)*512 + (k/8)*128.
 __device__ __forceinline__ uint32_t b_offset(int n, int k) {
-  return (uint32_t)((n >> 3) * 256 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2);
-}
-
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};\n" ::"r"(taddr), "r"(a), "r"(b),
-               "r"(c), "r"(d)
-               : "memory");
+  return (uint32_t)((n >> 3) * 512 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2);
 }
 
 __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_constant__ FaTcParams p) {
-  extern __shared__ __align__(1024) uint8_t smem[];  // 2 stages of [B_hi; B_lo]: 2 * 2 * NT * 16 bf16
+  extern __shared__ __align__(1024) uint8_t smem[];  // 2 stages of [B_hi; B_lo]: 2 * 2 * NT * 32 bf16
   __shared__ __align__(8) uint64_t empty[2];
   __shared__ __align__(8) uint64_t done;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t stage_bytes = 2u * p.NT * kKC * 2;
+  const uint32_t stage_bytes = 2u * p.NT * kKC * 2;  // [B_hi; B_lo], NT x 32 bf16 each
 
   int bid = blockIdx.x;
   const int mt = bid % p.mtiles;
@@ -89,7 +84,7 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
   const uint32_t tmem = tmem_slot;
   grid_dependency_wait();  // launched with programmatic serialisation: global memory only after this
 
-  // this thread's A element block: lane quarter (warp & 3), K half (warp >> 2)
+  // this thread's A elements: row m (lane quarter warp & 3), K half warp >> 2
   const int m = (warp & 3) * 32 + lane, khalf = warp >> 2;
   const int mg = mt * kMT + m;
   const bool mvalid = mg < p.M;
@@ -97,71 +92,100 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
   const int c = mvalid ? mg / ohw : 0, rs = mvalid ? mg - c * ohw : 0;
   const int r = rs / p.OW, s = rs - r * p.OW;
   // this thread's B elements: row n, K quarter
-  const int n = tid >> 2, kq = (tid & 3) * 4;
+  const int n = tid >> 2, kq = (tid & 3) * 8;
   const int l = nb * kNT + n;
   const bool nvalid = n < p.NT && l < p.L;
+  const float *xt = p.x + ((size_t)c * p.H + r) * p.W + s + khalf * 16;  // + b*C*H*W + i*W + j0
+  const float *gt = p.g + (size_t)(nvalid ? l : 0) * p.Hg * p.Wg;         // + b*L*Hg*Wg + row*Wg
+  const size_t ximg = (size_t)p.C * p.H * p.W, gimg = (size_t)p.L * p.Hg * p.Wg;
 
-  float ra[8], rb[4];
-  auto load = [&](int q) {
-    const int jb = q % p.jb, rest = q / p.jb;
-    const int i = rest % p.Hg, b = rest / p.Hg;
-    const int j0 = jb * kKC;
-    const float *xr = p.x + (((size_t)b * p.C + c) * p.H + (r + i)) * p.W + s;
+  // the next chunk to load, as (image lb, gradient row li, pixel block lj),
+  // advanced one chunk per load (no divisions in the loop)
+  int lj = q0 % p.jb, li = (q0 / p.jb) % p.Hg, lb = q0 / (p.jb * p.Hg);
+  float ra[kPF][16], rb[kPF][8];
+  auto load = [&](float (&a)[16], float (&bv)[8]) {
+    const int j0 = lj * kKC;
+    const float *xr = xt + lb * ximg + (size_t)li * p.W + j0;
+    const int ii = p.conv ? p.Hg - 1 - li : li;
+    const float *gr = gt + lb * gimg + (size_t)ii * p.Wg;
+    if (j0 + kKC <= p.Wg) {
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int j = j0 + khalf * 8 + e;
-      ra[e] = (mvalid && j < p.Wg) ? __ldg(xr + j) : 0.0f;
+      for (int e = 0; e < 16; ++e) a[e] = mvalid ? __ldg(xr + e) : 0.0f;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int j = j0 + kq + e;
+        bv[e] = nvalid ? __ldg(gr + (p.conv ? p.Wg - 1 - j : j)) : 0.0f;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) a[e] = (mvalid && j0 + khalf * 16 + e < p.Wg) ? __ldg(xr + e) : 0.0f;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int j = j0 + kq + e;
+        bv[e] = (nvalid && j < p.Wg) ? __ldg(gr + (p.conv ? p.Wg - 1 - j : j)) : 0.0f;
+      }
     }
-    const int ii = p.conv ? p.Hg - 1 - i : i;
-    const float *gr = p.g + (((size_t)b * p.L + l) * p.Hg + ii) * p.Wg;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const int j = j0 + kq + e;
-      rb[e] = (nvalid && j < p.Wg) ? __ldg(gr + (p.conv ? p.Wg - 1 - j : j)) : 0.0f;
+    if (++lj == p.jb) {
+      lj = 0;
+      if (++li == p.Hg) {
+        li = 0;
+        ++lb;
+      }
     }
   };
 
-  const uint32_t acc = tmem;                                  // [hh | small], 2 * NT columns
-  const uint32_t a_col0 = tmem + 2u * kNT;                    // stage st: hi at + 16 st, lo at + 8
+  const uint32_t acc = tmem;                  // [hh | small], 2 * NT columns
+  const uint32_t a_col0 = tmem + 2u * kNT;    // stage st: hi words at + 32 st, lo words at + 16
   const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
   const uint32_t idesc_n = idesc_bf16_f32(kMT, p.NT), idesc_2n = idesc_bf16_f32(kMT, 2 * p.NT);
   bool failed = false;
-  if (q0 < q1) load(q0);
-  for (int q = q0; q < q1; ++q) {
-    const int t = q - q0, st = t & 1;
-    if (t >= 2 && !mbar_wait(&empty[st], ((t >> 1) - 1) & 1, p.err)) failed = true;
-    if (__syncthreads_or(failed)) {
-      failed = true;
-      break;
-    }
-    // A: this thread's 8 values of row m -> 4 hi and 4 lo words
-    uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) split_bf16x2(ra[2 * e], ra[2 * e + 1], hi[e], lo[e]);
-    const uint32_t acol = a_col0 + 16u * st + 4u * khalf + lane_base;
-    tmem_st4(acol, hi[0], hi[1], hi[2], hi[3]);
-    tmem_st4(acol + 8, lo[0], lo[1], lo[2], lo[3]);
-    // B: this thread's 4 values of row n -> the hi and lo images of the stage
-    uint8_t *bst = smem + (size_t)st * stage_bytes;
-    if (n < p.NT) {
-      uint32_t bh[2], bl[2];
-      split_bf16x2(rb[0], rb[1], bh[0], bl[0]);
-      split_bf16x2(rb[2], rb[3], bh[1], bl[1]);
-      const uint32_t off = b_offset(n, kq);
-      *reinterpret_cast<uint2 *>(bst + off) = make_uint2(bh[0], bh[1]);
-      *reinterpret_cast<uint2 *>(bst + (size_t)p.NT * kKC * 2 + off) = make_uint2(bl[0], bl[1]);
-    }
-    if (q + 1 < q1) load(q + 1);  // in flight while this chunk is multiplied
-    tc_wait_st();
-    fence_proxy_async_smem();
-    tc_fence_before();
-    __syncthreads();
-    if (tid == 0) {
-      tc_fence_after();
-      const uint64_t dh = smem_desc_kmajor(smem_u32(bst), 128, 256);
-      mma_bf16_ts(acc, a_col0 + 16u * st, dh, idesc_2n, t > 0 ? 1u : 0u);  // [hi*hi | hi*lo]
-      mma_bf16_ts(acc + p.NT, a_col0 + 16u * st + 8, dh, idesc_n, 1u);     // small half += lo*hi
-      tc_commit(&empty[st]);
+  for (int u = 0; u < kPF; ++u)
+    if (q0 + u < q1) load(ra[u], rb[u]);
+  for (int qb = q0; qb < q1 && !failed; qb += kPF) {
+#pragma unroll
+    for (int u = 0; u < kPF; ++u) {
+      const int q = qb + u;
+      if (q >= q1) break;
+      const int t = q - q0, st = t & 1;
+      if (t >= 2 && !mbar_wait(&empty[st], ((t >> 1) - 1) & 1, p.err)) failed = true;
+      if (__syncthreads_or(failed)) {
+        failed = true;
+        break;
+      }
+      // A: this thread's 16 values of row m -> 8 hi and 8 lo words
+      uint32_t hi[8], lo[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) split_bf16x2(ra[u][2 * e], ra[u][2 * e + 1], hi[e], lo[e]);
+      const uint32_t acol = a_col0 + 32u * st + 8u * khalf + lane_base;
+      tmem_st8(acol, hi);
+      tmem_st8(acol + 16, lo);
+      // B: this thread's 8 values of row n -> the hi and lo images of the stage
+      uint8_t *bst = smem + (size_t)st * stage_bytes;
+      if (n < p.NT) {
+        uint32_t bh[4], bl[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) split_bf16x2(rb[u][2 * e], rb[u][2 * e + 1], bh[e], bl[e]);
+        const uint32_t off = b_offset(n, kq);
+        *reinterpret_cast<uint4 *>(bst + off) = make_uint4(bh[0], bh[1], bh[2], bh[3]);
+        *reinterpret_cast<uint4 *>(bst + (size_t)p.NT * kKC * 2 + off) = make_uint4(bl[0], bl[1], bl[2], bl[3]);
+      }
+      if (q + kPF < q1) load(ra[u], rb[u]);  // kPF chunks ahead
+      tc_wait_st();
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+#pragma unroll
+        for (int ks = 0; ks < kKC / 16; ++ks) {
+          const uint64_t dh = smem_desc_kmajor(smem_u32(bst) + 256u * ks, 128, 512);
+          const uint32_t ah = a_col0 + 32u * st + 8u * ks;
+          mma_bf16_ts(acc, ah, dh, idesc_2n, (t > 0 || ks > 0) ? 1u : 0u);  // [hi*hi | hi*lo]
+          mma_bf16_ts(acc + p.NT, ah + 16, dh, idesc_n, 1u);                // small half += lo*hi
+        }
+        tc_commit(&empty[st]);
+      }
     }
   }
   // every MMA issued has retired before the accumulator is read or freed
@@ -224,7 +248,7 @@ FaTcParams make_params(const ConvGeom &g, int sms) {
   p.jb = (p.Wg + kKC - 1) / kKC;
   p.nch = p.B * p.Hg * p.jb;
   const int tiles = p.mtiles * p.nblocks;
-  int splits = (2 * sms + tiles - 1) / tiles;  // about two CTAs per SM
+  int splits = (2 * sms) / tiles;  // two CTAs per SM: one wave
   splits = std::max(1, std::min(splits, p.nch));
   p.splits = splits;
   return p;
@@ -258,7 +282,7 @@ int launch_fa_tc(const ConvGeom &g, const float *x, const float *f, float *y, fl
   if (!work) return set_error(CCT_EINVAL, "tensor-core FilterAdjoint needs plan workspace");
   const long long grid = (long long)p.mtiles * p.nblocks * p.splits;
   if (grid > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "FilterAdjoint grid too large");
-  // the stages need 2 * 2 * NT * 16 bf16 (8 KB at most); asking for 96 KB keeps
+  // the stages need 2 * 2 * NT * 32 bf16 (16 KB at most); asking for 96 KB keeps
   // at most two CTAs on an SM, so their tensor memory (256 columns each)
   // always fits and no allocation waits
   const size_t smem = 96 * 1024;

@@ -21,7 +21,7 @@
 // sums; fa_tc_reduce adds the splits in split order, so the result does not
 // depend on scheduling.  Within a CTA all 8 warps build every chunk (the
 // next chunk's loads in flight while the current one is converted and
-// multiplied) into one of two stages; one thread issues the MMAs, whose
+// multiplied) into one of kStages stages; one thread issues the MMAs, whose
 // commit frees the stage.  Every wait is bounded; on a timeout the CTA
 // raises the device error word, waits (bounded) for its MMAs, frees its
 // tensor memory and leaves.
@@ -41,6 +41,7 @@ constexpr int kNT = 64;    // gradient planes per column block (max)
 constexpr int kKC = 32;    // gradient pixels per reduction chunk (two MMA K-steps)
 constexpr int kTmemCols = 256;
 constexpr int kPF = 2;     // chunks whose loads are in flight ahead of the one being built
+constexpr int kStages = 4; // A/B stages: chunks built ahead of the MMAs that read them
 
 struct FaTcParams {
   int H, W, Hg, Wg, OH, OW, C, L, B;
@@ -58,8 +59,8 @@ __device__ __forceinline__ uint32_t b_offset(int n, int k) {
 }
 
 __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_constant__ FaTcParams p) {
-  extern __shared__ __align__(1024) uint8_t smem[];  // 2 stages of [B_hi; B_lo]: 2 * 2 * NT * 32 bf16
-  __shared__ __align__(8) uint64_t empty[2];
+  extern __shared__ __align__(1024) uint8_t smem[];  // kStages stages of [B_hi; B_lo]: 2 * NT * 32 bf16 each
+  __shared__ __align__(8) uint64_t empty[kStages];
   __shared__ __align__(8) uint64_t done;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -72,8 +73,7 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
   const int q0 = (int)((long long)split * p.nch / p.splits), q1 = (int)((long long)(split + 1) * p.nch / p.splits);
 
   if (tid == 0) {
-    mbar_init(&empty[0], 1);
-    mbar_init(&empty[1], 1);
+    for (int k = 0; k < kStages; ++k) mbar_init(&empty[k], 1);
     mbar_init(&done, 1);
     fence_barrier_init();
   }
@@ -147,8 +147,8 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
     for (int u = 0; u < kPF; ++u) {
       const int q = qb + u;
       if (q >= q1) break;
-      const int t = q - q0, st = t & 1;
-      if (t >= 2 && !mbar_wait(&empty[st], ((t >> 1) - 1) & 1, p.err)) failed = true;
+      const int t = q - q0, st = t % kStages;
+      if (t >= kStages && !mbar_wait(&empty[st], ((t / kStages) - 1) & 1, p.err)) failed = true;
       if (__syncthreads_or(failed)) {
         failed = true;
         break;
@@ -282,11 +282,12 @@ int launch_fa_tc(const ConvGeom &g, const float *x, const float *f, float *y, fl
   if (!work) return set_error(CCT_EINVAL, "tensor-core FilterAdjoint needs plan workspace");
   const long long grid = (long long)p.mtiles * p.nblocks * p.splits;
   if (grid > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "FilterAdjoint grid too large");
-  // the stages need 2 * 2 * NT * 32 bf16 (16 KB at most); asking for 96 KB keeps
+  // the stages need kStages * 2 * NT * 32 bf16 (32 KB at most); asking for 96 KB keeps
   // at most two CTAs on an SM, so their tensor memory (256 columns each)
   // always fits and no allocation waits
   const size_t smem = 96 * 1024;
-  static_assert(2u * 2u * kNT * kKC * 2 <= 96 * 1024, "FilterAdjoint stages");
+  static_assert(kStages * 2u * kNT * kKC * 2 <= 96 * 1024, "FilterAdjoint stages");
+  static_assert(2 * kNT + kStages * kKC <= kTmemCols, "FilterAdjoint tensor memory");
   int rc = check_cuda(cudaFuncSetAttribute(fa_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
                       "cudaFuncSetAttribute(fa_tc)");
   if (rc) return rc;

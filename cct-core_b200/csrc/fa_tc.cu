@@ -149,7 +149,9 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
       if (q >= q1) break;
       const int t = q - q0, st = t % kStages;
       if (t >= kStages && !mbar_wait(&empty[st], ((t / kStages) - 1) & 1, p.err)) failed = true;
-      if (__syncthreads_or(failed)) {
+      // the CTA agrees on a timeout once per kStages chunks (a late stop only
+      // spoils results that the device status already reports as failed)
+      if (st == 0 && __syncthreads_or(failed)) {
         failed = true;
         break;
       }

@@ -20,9 +20,10 @@
 // contiguous range of chunks into its accumulator and stores its partial
 // sums; fa_tc_reduce adds the splits in split order, so the result does not
 // depend on scheduling.  Within a CTA all 8 warps build every chunk (the
-// next chunk's loads in flight while the current one is converted and
-// multiplied) into one of kStages stages; one thread issues the MMAs, whose
-// commit frees the stage.  Every wait is bounded; on a timeout the CTA
+// next chunks' loads in flight while the current one is converted) into one
+// of kStages stages and arrive on the stage's `full` barrier; one thread
+// waits on it, issues the MMAs, and their commit on `empty` frees the stage.
+// Every wait is bounded; on a timeout the CTA
 // raises the device error word, waits (bounded) for its MMAs, frees its
 // tensor memory and leaves.
 #include <cuda_bf16.h>
@@ -61,6 +62,7 @@ __device__ __forceinline__ uint32_t b_offset(int n, int k) {
 __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_constant__ FaTcParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];  // kStages stages of [B_hi; B_lo]: 2 * NT * 32 bf16 each
   __shared__ __align__(8) uint64_t empty[kStages];
+  __shared__ __align__(8) uint64_t full[kStages];
   __shared__ __align__(8) uint64_t done;
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -73,7 +75,10 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
   const int q0 = (int)((long long)split * p.nch / p.splits), q1 = (int)((long long)(split + 1) * p.nch / p.splits);
 
   if (tid == 0) {
-    for (int k = 0; k < kStages; ++k) mbar_init(&empty[k], 1);
+    for (int k = 0; k < kStages; ++k) {
+      mbar_init(&empty[k], 1);                // the MMA commit
+      mbar_init(&full[k], kFaThreads / 32);   // one arrival per warp
+    }
     mbar_init(&done, 1);
     fence_barrier_init();
   }
@@ -173,20 +178,27 @@ __global__ void __launch_bounds__(kFaThreads, 2) fa_tc_kernel(const __grid_const
         *reinterpret_cast<uint4 *>(bst + (size_t)p.NT * kKC * 2 + off) = make_uint4(bl[0], bl[1], bl[2], bl[3]);
       }
       if (q + kPF < q1) load(ra[u], rb[u]);  // kPF chunks ahead
+      // this warp's part of the chunk is in place: tensor-memory stores done,
+      // shared-memory stores visible to the tensor core's (async) proxy
       tc_wait_st();
       fence_proxy_async_smem();
       tc_fence_before();
-      __syncthreads();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&full[st]);
       if (tid == 0) {
+        const bool ready = mbar_wait(&full[st], (t / kStages) & 1, p.err);
+        if (!ready) failed = true;
         tc_fence_after();
+        if (ready) {
 #pragma unroll
-        for (int ks = 0; ks < kKC / 16; ++ks) {
-          const uint64_t dh = smem_desc_kmajor(smem_u32(bst) + 256u * ks, 128, 512);
-          const uint32_t ah = a_col0 + 32u * st + 8u * ks;
-          mma_bf16_ts(acc, ah, dh, idesc_2n, (t > 0 || ks > 0) ? 1u : 0u);  // [hi*hi | hi*lo]
-          mma_bf16_ts(acc + p.NT, ah + 16, dh, idesc_n, 1u);                // small half += lo*hi
+          for (int ks = 0; ks < kKC / 16; ++ks) {
+            const uint64_t dh = smem_desc_kmajor(smem_u32(bst) + 256u * ks, 128, 512);
+            const uint32_t ah = a_col0 + 32u * st + 8u * ks;
+            mma_bf16_ts(acc, ah, dh, idesc_2n, (t > 0 || ks > 0) ? 1u : 0u);  // [hi*hi | hi*lo]
+            mma_bf16_ts(acc + p.NT, ah + 16, dh, idesc_n, 1u);                // small half += lo*hi
+          }
         }
-        tc_commit(&empty[st]);
+        tc_commit(&empty[st]);  // frees the stage once the MMAs issued so far are done
       }
     }
   }

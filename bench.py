@@ -347,6 +347,32 @@ def plain_workload():
                                                _lib.BORDER_ZERO, _lib.CONVOLUTION, tmp.data_ptr(),
                                                y.data_ptr(), ctypes.c_void_p(stream)))
     sep_s = time_single_launch(separable, reps=10)
+
+    def other_ops():
+        """The other convolution operators beside the batched convolve: a
+        1024x1024 ScalarField cross-correlated with an 8x8 MatrixField of 7x7
+        matrices (64 output planes), and a 2048x2048 ColorField (RGBA8)
+        convolved with a 5x5 filter (unpack, three planes, pack)."""
+        sm_x = torch.empty((1024, 1024), device="cuda").uniform_(-1, 1, generator=gen)
+        sm_m = torch.empty((7, 7, 8, 8), device="cuda").uniform_(-1, 1, generator=gen)
+        sm_y = torch.empty((64, 1024, 1024), device="cuda")
+
+        def scalar_matrix():
+            _lib.check(_lib.LIB.cct_conv_scalar_matrix(1024, 1024, sm_x.data_ptr(), sm_m.data_ptr(), 8, 8, 7,
+                                                       _lib.BORDER_ZERO, _lib.CROSS_CORRELATION,
+                                                       _lib.SAMPLE_NONE, 1, sm_y.data_ptr(),
+                                                       ctypes.c_void_p(stream)))
+        t_sm = time_single_launch(scalar_matrix, reps=10)
+        img = torch.randint(0, 256, (2048, 2048, 4), dtype=torch.uint8, device="cuda", generator=gen)
+        out = torch.empty_like(img)
+        cplan = _lib.ColorPlan(C.make_desc((2048, 2048, 0), (5, 5, 0), C.BorderZero, _lib.CONVOLUTION,
+                                           C.NoSamplingConvolution, _lib.PLANE_BY_PLANE))
+        cf = torch.empty((5, 5), device="cuda").uniform_(0, 0.08, generator=gen)
+        t_c = time_single_launch(lambda: cplan.run(img.data_ptr(), cf.data_ptr(), out.data_ptr(), stream), reps=10)
+        cplan.close()
+        return {"ms": round(t_sm * 1e3, 4), "GFLOP/s": round(2 * 1024 * 1024 * 64 * 49 / t_sm / 1e9, 1),
+                "color": {"ms": round(t_c * 1e3, 4),
+                          "pixels/s": round(2048 * 2048 / t_c, 1)}}
     sep_bytes = 2 * 4 * P * H * W
     step()
     torch.cuda.synchronize()
@@ -354,7 +380,9 @@ def plain_workload():
     extra = {"error_vs_fp64": dict(errors_vs(y[:1].cpu().numpy(), ref), sample="plane 0"),
              "single_plane_256x256_us": round(single_s * 1e6, 2),
              "separable_5+5_4096x256x256": {"ms": round(sep_s * 1e3, 4),
-                                            "GB/s": round(sep_bytes / sep_s / 1e9, 1)}}
+                                            "GB/s": round(sep_bytes / sep_s / 1e9, 1)},
+             "scalar_matrix_1024x1024_8x8_of_7x7": other_ops()}
+    extra["color_2048x2048_5x5"] = extra["scalar_matrix_1024x1024_8x8_of_7x7"].pop("color")
 
     byts = 4 * (2 * P * H * W + R * R)
     return {

@@ -18,6 +18,13 @@ beside it); serve (10,000 seeded convolve/projectFrame requests of uneven
 sizes with Poisson arrivals, served with continuous batching and with plain
 per-call dispatch: throughput and p50/p99 latency, rate swept 1k-50k/s).
 
+Beside the headline each line carries: max/RMS error against an FP64
+reference (error_vs_fp64), and per workload the neighbouring operators --
+frame: the same layer's weight gradient (FilterAdjointBlockReduceSum, FP32 and
+split BF16); plain: one 256x256 plane alone, the separable form, a
+ScalarField (*) MatrixField and a ColorField convolution; fft: the direct
+kernel and a dynamic filter; graph: batches 1, 8 and 64 in both precisions.
+
 Prints one JSON line (rank 0).  Multi-GPU: replicas only -- every rank runs
 the same step on its own GPU; value = all ranks' work / max rank time.
 """

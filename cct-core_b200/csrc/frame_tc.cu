@@ -27,8 +27,9 @@
 //                so NT <= 64.
 //   warp 17    loader: 3-D TMA loads of the halo tile (zero fill at the
 //              border) and bulk copies of the pre-packed filter chunks.
-//   warps 18-21 epilogue: tcgen05.ld of the accumulator, optional ReLU,
-//              coalesced stores to the output planes.
+//   warps 18-25 epilogue, two per tensor-memory lane quarter taking
+//              alternate 16-column blocks: tcgen05.ld of the accumulator,
+//              optional ReLU, coalesced stores to the output planes.
 // Every mbarrier wait is bounded; on a timeout the CTA raises the device
 // error word, lets in-flight copies land, frees its tensor memory and exits.
 #include <cuda_bf16.h>
@@ -49,8 +50,9 @@ constexpr int kStages = 8;      // A/B chunk pipeline depth
 constexpr int kGroups = 4;      // producer groups: group j builds chunks q = j (mod kGroups)
 constexpr int kProdWarps = 4 * kGroups;
 constexpr int kProdThreads = 32 * kProdWarps;
-constexpr int kMmaWarp = kProdWarps, kLoadWarp = kProdWarps + 1;  // then 4 epilogue warps
-constexpr int kThreads = 32 * (kProdWarps + 6);
+constexpr int kMmaWarp = kProdWarps, kLoadWarp = kProdWarps + 1;  // then the epilogue warps
+constexpr int kEpiWarps = 8;  // two per lane quarter: the last tile's epilogue is the launch's tail
+constexpr int kThreads = 32 * (kProdWarps + 2 + kEpiWarps);
 static_assert(kStages % kGroups == 0, "a stage must always belong to the same producer group");
 
 // Byte offset of element (n, k) inside one packed K-major operand image of
@@ -99,7 +101,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_init(&bars.hempty[0], kProdWarps);  // halo block converted (one arrival per producer warp)
     for (int h = 0; h < 2; ++h) {
       mbar_init(&bars.dfull[h], 1);
-      mbar_init(&bars.dempty[h], 4);  // one arrival per epilogue warp
+      mbar_init(&bars.dempty[h], kEpiWarps);  // one arrival per epilogue warp
     }
     mbar_init(&bars.drain, 1);
     bars.abort_flag = 0;
@@ -322,6 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else {
     // ------------------------------------------------------------ epilogue
     const int sub = warp & 3;  // TMEM lane quarter this warp may access
+    const int half = (warp - (kProdWarps + 2)) >> 2;  // which alternate 16-column blocks
     const int m = sub * 32 + lane;
     const uint32_t lane_base = (uint32_t)(sub * 32) << 16;
     const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
@@ -341,7 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       const bool valid = pix < npix;
       const int n0 = nb * p.NT;
       float *ybase = p.y + ((size_t)b * g.groups + n0) * npix + pix;
-      for (int c = 0; c < p.NT; c += 16) {
+      for (int c = 16 * half; c < p.NT; c += 32) {
         uint32_t v[16], v2[16];
         tmem_ld16(tmem + lane_base + d_col(d) + c, v);
         tmem_ld16(tmem + lane_base + d_col(d) + p.NT + c, v2);

@@ -21,10 +21,11 @@
 //                A_lo x B_hi (N = NT) into the second half, so the two
 //                small products never meet the large hi*hi sum (the tensor
 //                core's FP32 accumulation would round them against it);
-//                the epilogue adds the halves.  A tcgen05.mma costs ~46
-//                cycles however narrow, so the wide first MMA pays.  The
-//                double-buffered [hh | small] accumulator is 4*NT columns,
-//                so NT <= 64.
+//                the epilogue adds the halves.  The concatenated first MMA
+//                reads A_hi once for both products and halves the
+//                instruction count (the tensor time is N/2 cycles per MMA
+//                either way).  The double-buffered [hh | small]
+//                accumulator is 4*NT columns, so NT <= 64.
 //   warp 17    loader: 3-D TMA loads of the halo tile (zero fill at the
 //              border) and bulk copies of the pre-packed filter chunks.
 //   warps 18-25 epilogue, two per tensor-memory lane quarter taking

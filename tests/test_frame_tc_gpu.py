@@ -82,6 +82,8 @@ TC_CASES = [
     (56, 56, 32, 32, 1, 1, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
     (16, 16, 32, 16, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
     (44, 48, 24, 72, 2, 5, O.ZERO, O.DOWN, 2, O.BACKPROJECT_REDUCE),
+    # a 208-wide halo: 16-plane blocks (two 32-plane halo buffers do not fit)
+    (24, 200, 32, 64, 1, 5, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
 ]
 
 

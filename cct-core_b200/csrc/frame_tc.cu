@@ -15,8 +15,10 @@
 //              j copies, for every chunk q = j (mod 4), the pixel's split
 //              words of that tap into the chunk's tensor-memory stage
 //              (tcgen05.st, row m = lane m): four chunks are in flight.
-//   warp 16    MMA issuer (one elected lane): per 16-deep k-step of a chunk,
-//              with A from tensor memory and B from shared memory,
+//   warp 16    MMA issuer: the warp probes the next 8 chunks at once and
+//              issues every ready one in a batch; one elected lane issues,
+//              per 16-deep k-step of a chunk, with A from tensor memory and
+//              B from shared memory,
 //                A_hi x [B_hi; B_lo] (N = 2*NT) into [hh | small], then
 //                A_lo x B_hi (N = NT) into the second half, so the two
 //                small products never meet the large hi*hi sum (the tensor
@@ -27,7 +29,10 @@
 //                either way).  The double-buffered [hh | small]
 //                accumulator is 4*NT columns, so NT <= 64.
 //   warp 17    loader: 3-D TMA loads of the halo tile (zero fill at the
-//              border) and bulk copies of the pre-packed filter chunks.
+//              border) and bulk copies of the pre-packed filter chunks; the
+//              warp probes the next 8 stages at once and each lane issues the
+//              copy of one free stage, so a batch of copies goes out together
+//              (one thread looping over them issued one per ~480 cycles).
 //   warps 18-25 epilogue, two per tensor-memory lane quarter taking
 //              alternate 16-column blocks: tcgen05.ld of the accumulator,
 //              optional ReLU, coalesced stores to the output planes.

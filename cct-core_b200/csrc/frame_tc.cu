@@ -57,6 +57,11 @@ constexpr int kGroups = 4;      // producer groups: group j builds chunks q = j 
 constexpr int kProdWarps = 4 * kGroups;
 constexpr int kProdThreads = 32 * kProdWarps;
 constexpr int kMmaWarp = kProdWarps, kLoadWarp = kProdWarps + 1;  // then the epilogue warps
+// Filters of at least this many taps use the batched MMA issuer and the
+// warp-wide loader; smaller ones (3x3: 9-chunk blocks) keep one chunk per
+// loop trip, which measured faster for them (an eight-layer 3x3 stack: 5.3
+// against 6.3 ms per step; 5x5 filter banks: 0.097 against 0.091 ms).
+constexpr int kBatchTaps = 16;
 constexpr int kEpiWarps = 8;  // two per lane quarter: the last tile's epilogue is the launch's tail
 constexpr int kThreads = 32 * (kProdWarps + 2 + kEpiWarps);
 static_assert(kStages % kGroups == 0, "a stage must always belong to the same producer group");
@@ -240,40 +245,64 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_fence_after();
       const uint32_t dt = tmem + d_col(d);
       const int nchunks = p.NCB * RS;
-      for (int k = 0; k < nchunks;) {
-        // Lane i probes chunk q + i; every chunk ready in order from q is
-        // issued in one batch, so the barrier probe, the vote and the fence
-        // are paid once per batch instead of once per chunk.  A stage is at
-        // most one phase ahead of this warp (its producers need the MMAs of
-        // the chunk kStages earlier), so the parity test is exact.
-        const bool ready = lane < kStages && k + lane < nchunks &&
-                           mbar_test(&bars.full[(q + lane) % kStages], ((q + lane) / kStages) & 1);
-        int nready = __ffs(~__ballot_sync(0xffffffffu, ready)) - 1;
-        if (nready == 0) {
-          failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[q % kStages], (q / kStages) & 1, p.err));
-          if (failed) break;
-          nready = 1;
+      if (RS >= kBatchTaps) {
+        for (int k = 0; k < nchunks;) {
+          // Lane i probes chunk q + i; every chunk ready in order from q is
+          // issued in one batch, so the barrier probe, the vote and the fence
+          // are paid once per batch instead of once per chunk.  A stage is at
+          // most one phase ahead of this warp (its producers need the MMAs of
+          // the chunk kStages earlier), so the parity test is exact.
+          const bool ready = lane < kStages && k + lane < nchunks &&
+                             mbar_test(&bars.full[(q + lane) % kStages], ((q + lane) / kStages) & 1);
+          int nready = __ffs(~__ballot_sync(0xffffffffu, ready)) - 1;
+          if (nready == 0) {
+            failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[q % kStages], (q / kStages) & 1, p.err));
+            if (failed) break;
+            nready = 1;
+          }
+          tc_fence_after();
+          if (elect_one()) {
+            for (int i = 0; i < nready; ++i) {
+              const uint32_t s = (q + i) % kStages;
+              const uint32_t a_hi = tmem + a_col0 + s * CB;
+              const uint32_t a_lo = a_hi + CB / 2;
+              const uint32_t b_hi = bstage0 + s * bstage_bytes;
+#pragma unroll
+              for (int j = 0; j < CB / 16; ++j) {
+                const uint32_t acc = (k + i > 0 || j > 0) ? 1u : 0u;
+                const uint64_t dh = smem_desc_kmajor(b_hi + 256u * j, lbo, sbo);
+                mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_2n, acc);       // [hi*hi | hi*lo]
+                mma_bf16_ts(dt + p.NT, a_lo + 8u * j, dh, idesc_n, 1u);  // small half += lo*hi
+              }
+              tc_commit(&bars.empty[s]);
+            }
+          }
+          __syncwarp();
+          k += nready;
+          q += nready;
         }
-        tc_fence_after();
-        if (elect_one()) {
-          for (int i = 0; i < nready; ++i) {
-            const uint32_t s = (q + i) % kStages;
-            const uint32_t a_hi = tmem + a_col0 + s * CB;
-            const uint32_t a_lo = a_hi + CB / 2;
-            const uint32_t b_hi = bstage0 + s * bstage_bytes;
+      } else {
+        // one chunk per probe (filters of fewer taps: short blocks)
+        for (int k = 0; k < nchunks; ++k, ++q) {
+          const int s = q % kStages;
+          failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[s], (q / kStages) & 1, p.err));
+          if (failed) break;
+          tc_fence_after();
+          const uint32_t a_hi = tmem + a_col0 + (uint32_t)s * CB;
+          const uint32_t a_lo = a_hi + CB / 2;
+          const uint32_t b_hi = bstage0 + (uint32_t)s * bstage_bytes;
+          if (elect_one()) {
 #pragma unroll
             for (int j = 0; j < CB / 16; ++j) {
-              const uint32_t acc = (k + i > 0 || j > 0) ? 1u : 0u;
+              const uint32_t acc = (k > 0 || j > 0) ? 1u : 0u;
               const uint64_t dh = smem_desc_kmajor(b_hi + 256u * j, lbo, sbo);
               mma_bf16_ts(dt, a_hi + 8u * j, dh, idesc_2n, acc);       // [hi*hi | hi*lo]
               mma_bf16_ts(dt + p.NT, a_lo + 8u * j, dh, idesc_n, 1u);  // small half += lo*hi
             }
             tc_commit(&bars.empty[s]);
           }
+          __syncwarp();
         }
-        __syncwarp();
-        k += nready;
-        q += nready;
       }
       if (failed) break;
       if (elect_one()) tc_commit(&bars.dfull[d]);
@@ -286,81 +315,139 @@ __global__ void __launch_bounds__(kThreads, 1)
     mbar_wait(&bars.drain, 0, p.err);
   } else if (warp == kLoadWarp) {
     // ------------------------------------------------------------ loader
-    // The whole warp walks the chunks (its values stay warp-uniform).  Lane i
-    // probes the stage of chunk q + i; every chunk whose stage is free, in
-    // order from q, has its filter copy issued at once by its own lane, so the
-    // copies of a batch go out together instead of one loop trip each.  A
-    // stage is at most one phase ahead of this warp (its next MMA needs this
-    // warp's copy), so the parity test is exact.  Lane 0 alone issues the
-    // halo blocks; every lane keeps the same bookkeeping.
-    const uint32_t halo_tx = (uint32_t)(p.TC * p.TR * CB * 4);
-    // Halo blocks in the producers' order: (tile, cb) for this CTA's tiles.
-    int h_tile = blockIdx.x, h_cb = 0;  // next halo block to issue
-    uint32_t h_issued = 0;
-    auto halo_try = [&](bool block) -> int {
-      // 1 issued, 0 not yet possible, -1 timed out (warp-uniform)
-      if (h_tile >= p.total_tiles) return 0;
-      const uint32_t parity = (h_issued & 1) ^ 1;
-      int st = 0;
-      if (lane == 0) st = block ? (mbar_wait(&bars.hempty[0], parity, p.err) ? 1 : -1)
-                                : (mbar_test(&bars.hempty[0], parity) ? 1 : 0);
-      st = __shfl_sync(0xffffffffu, st, 0);
-      if (st <= 0) return st;
-      if (lane == 0) {
+    if (RS >= kBatchTaps) {
+      // The whole warp walks the chunks (its values stay warp-uniform).  Lane i
+      // probes the stage of chunk q + i; every chunk whose stage is free, in
+      // order from q, has its filter copy issued at once by its own lane, so the
+      // copies of a batch go out together instead of one loop trip each.  A
+      // stage is at most one phase ahead of this warp (its next MMA needs this
+      // warp's copy), so the parity test is exact.  Lane 0 alone issues the
+      // halo blocks; every lane keeps the same bookkeeping.
+      const uint32_t halo_tx = (uint32_t)(p.TC * p.TR * CB * 4);
+      // Halo blocks in the producers' order: (tile, cb) for this CTA's tiles.
+      int h_tile = blockIdx.x, h_cb = 0;  // next halo block to issue
+      uint32_t h_issued = 0;
+      auto halo_try = [&](bool block) -> int {
+        // 1 issued, 0 not yet possible, -1 timed out (warp-uniform)
+        if (h_tile >= p.total_tiles) return 0;
+        const uint32_t parity = (h_issued & 1) ^ 1;
+        int st = 0;
+        if (lane == 0) st = block ? (mbar_wait(&bars.hempty[0], parity, p.err) ? 1 : -1)
+                                  : (mbar_test(&bars.hempty[0], parity) ? 1 : 0);
+        st = __shfl_sync(0xffffffffu, st, 0);
+        if (st <= 0) return st;
+        if (lane == 0) {
+          int b, mt, nb;
+          tile_decode(h_tile, b, mt, nb);
+          const int row0 = ((mt * kMT) / g.OW) * g.down - g.low_r;
+          mbar_arrive_expect_tx(&bars.hfull[0], halo_tx);
+          tma_load_3d(landing, &xmap, &bars.hfull[0], p.start_c, row0, b * g.n + h_cb * CB);
+        }
+        ++h_issued;
+        if (++h_cb == p.NCB) {
+          h_cb = 0;
+          h_tile += gridDim.x;
+        }
+        return 1;
+      };
+      bool ok = halo_try(true) >= 0;
+      uint32_t q = 0, hb = 0;
+      for (int i = blockIdx.x; ok && i < p.total_tiles && !__any_sync(0xffffffffu, *abort_flag != 0);
+           i += gridDim.x) {
+        int b, mt, nb;
+        tile_decode(i, b, mt, nb);
+        for (int cb = 0; ok && cb < p.NCB; ++cb, ++hb) {
+          const uint8_t *bsrc = p.bpack + (((size_t)nb * p.NCB + cb) * RS) * bstage_bytes;
+          for (int tap = 0; tap < RS;) {
+            const bool free_stage = lane < kStages && tap + lane < RS &&
+                                    mbar_test(&bars.empty[(q + lane) % kStages], (((q + lane) / kStages) & 1) ^ 1);
+            int n = __ffs(~__ballot_sync(0xffffffffu, free_stage)) - 1;
+            if (n == 0) {
+              ok = !__any_sync(0xffffffffu,
+                               lane == 0 && !mbar_wait(&bars.empty[q % kStages], ((q / kStages) & 1) ^ 1, p.err));
+              if (!ok) break;
+              n = 1;
+            }
+            if (lane < n) {
+              const uint32_t s = (q + lane) % kStages;
+              mbar_arrive_expect_tx(&bars.full[s], bstage_bytes);
+              bulk_load(bstage + (size_t)s * bstage_bytes, bsrc + (size_t)(tap + lane) * bstage_bytes, bstage_bytes,
+                        &bars.full[s]);
+            }
+            q += n;
+            tap += n;
+            // prefetch the next halo block as soon as the landing buffer is free
+            if (h_issued == hb + 1 && halo_try(false) < 0) ok = false;
+          }
+          // the producers need the next block before they can go on
+          if (ok && h_issued == hb + 1 && halo_try(true) < 0) ok = false;
+        }
+      }
+      if (!ok) *abort_flag = 1;
+      if (__any_sync(0xffffffffu, *abort_flag != 0) && lane == 0) {
+        // Let copies that may still be in flight land before this CTA's
+        // shared memory is released: the last kStages filter chunks and the
+        // last halo block issued.
+        for (uint32_t qq = q > kStages ? q - kStages : 0; qq < q; ++qq)
+          mbar_wait(&bars.full[qq % kStages], (qq / kStages) & 1, p.err);
+        if (h_issued > 0) mbar_wait(&bars.hfull[0], (h_issued - 1) & 1, p.err);
+      }
+    } else if (lane == 0) {
+      // one thread, one chunk per loop trip (filters of fewer taps)
+      const uint32_t halo_tx = (uint32_t)(p.TC * p.TR * CB * 4);
+      // Halo blocks in the producers' order: (tile, cb) for this CTA's tiles.
+      int h_tile = blockIdx.x, h_cb = 0;  // next halo block to issue
+      uint32_t h_issued = 0;
+      auto halo_ready_to_issue = [&](bool block) -> int {
+        // 1 issued, 0 not yet possible, -1 timed out
+        if (h_tile >= p.total_tiles) return 0;
+        const uint32_t parity = (h_issued & 1) ^ 1;
+        if (block) {
+          if (!mbar_wait(&bars.hempty[0], parity, p.err)) return -1;
+        } else if (!mbar_test(&bars.hempty[0], parity)) {
+          return 0;
+        }
         int b, mt, nb;
         tile_decode(h_tile, b, mt, nb);
         const int row0 = ((mt * kMT) / g.OW) * g.down - g.low_r;
         mbar_arrive_expect_tx(&bars.hfull[0], halo_tx);
         tma_load_3d(landing, &xmap, &bars.hfull[0], p.start_c, row0, b * g.n + h_cb * CB);
-      }
-      ++h_issued;
-      if (++h_cb == p.NCB) {
-        h_cb = 0;
-        h_tile += gridDim.x;
-      }
-      return 1;
-    };
-    bool ok = halo_try(true) >= 0;
-    uint32_t q = 0, hb = 0;
-    for (int i = blockIdx.x; ok && i < p.total_tiles && !__any_sync(0xffffffffu, *abort_flag != 0);
-         i += gridDim.x) {
-      int b, mt, nb;
-      tile_decode(i, b, mt, nb);
-      for (int cb = 0; ok && cb < p.NCB; ++cb, ++hb) {
-        const uint8_t *bsrc = p.bpack + (((size_t)nb * p.NCB + cb) * RS) * bstage_bytes;
-        for (int tap = 0; tap < RS;) {
-          const bool free_stage = lane < kStages && tap + lane < RS &&
-                                  mbar_test(&bars.empty[(q + lane) % kStages], (((q + lane) / kStages) & 1) ^ 1);
-          int n = __ffs(~__ballot_sync(0xffffffffu, free_stage)) - 1;
-          if (n == 0) {
-            ok = !__any_sync(0xffffffffu,
-                             lane == 0 && !mbar_wait(&bars.empty[q % kStages], ((q / kStages) & 1) ^ 1, p.err));
-            if (!ok) break;
-            n = 1;
-          }
-          if (lane < n) {
-            const uint32_t s = (q + lane) % kStages;
-            mbar_arrive_expect_tx(&bars.full[s], bstage_bytes);
-            bulk_load(bstage + (size_t)s * bstage_bytes, bsrc + (size_t)(tap + lane) * bstage_bytes, bstage_bytes,
-                      &bars.full[s]);
-          }
-          q += n;
-          tap += n;
-          // prefetch the next halo block as soon as the landing buffer is free
-          if (h_issued == hb + 1 && halo_try(false) < 0) ok = false;
+        ++h_issued;
+        if (++h_cb == p.NCB) {
+          h_cb = 0;
+          h_tile += gridDim.x;
         }
-        // the producers need the next block before they can go on
-        if (ok && h_issued == hb + 1 && halo_try(true) < 0) ok = false;
+        return 1;
+      };
+      bool ok = halo_ready_to_issue(true) >= 0;
+      uint32_t q = 0, hb = 0;
+      for (int i = blockIdx.x; ok && i < p.total_tiles && !*abort_flag; i += gridDim.x) {
+        int b, mt, nb;
+        tile_decode(i, b, mt, nb);
+        for (int cb = 0; ok && cb < p.NCB; ++cb, ++hb) {
+          const uint8_t *bsrc = p.bpack + (((size_t)nb * p.NCB + cb) * RS) * bstage_bytes;
+          for (int tap = 0; tap < RS; ++tap, ++q) {
+            const int s = q % kStages;
+            if (!mbar_wait(&bars.empty[s], ((q / kStages) & 1) ^ 1, p.err)) { ok = false; break; }
+            mbar_arrive_expect_tx(&bars.full[s], bstage_bytes);
+            bulk_load(bstage + (size_t)s * bstage_bytes, bsrc + (size_t)tap * bstage_bytes, bstage_bytes,
+                      &bars.full[s]);
+            // prefetch the next halo block as soon as the landing buffer is free
+            if (h_issued == hb + 1 && halo_ready_to_issue(false) < 0) ok = false;
+          }
+          // the producers need the next block before they can go on
+          if (ok && h_issued == hb + 1 && halo_ready_to_issue(true) < 0) ok = false;
+        }
       }
-    }
-    if (!ok) *abort_flag = 1;
-    if (__any_sync(0xffffffffu, *abort_flag != 0) && lane == 0) {
-      // Let copies that may still be in flight land before this CTA's
-      // shared memory is released: the last kStages filter chunks and the
-      // last halo block issued.
-      for (uint32_t qq = q > kStages ? q - kStages : 0; qq < q; ++qq)
-        mbar_wait(&bars.full[qq % kStages], (qq / kStages) & 1, p.err);
-      if (h_issued > 0) mbar_wait(&bars.hfull[0], (h_issued - 1) & 1, p.err);
+      if (!ok) *abort_flag = 1;
+      if (*abort_flag) {
+        // Let copies that may still be in flight land before this CTA's
+        // shared memory is released: the last kStages filter chunks and the
+        // last halo block issued.
+        for (uint32_t qq = q > kStages ? q - kStages : 0; qq < q; ++qq)
+          mbar_wait(&bars.full[qq % kStages], (qq / kStages) & 1, p.err);
+        if (h_issued > 0) mbar_wait(&bars.hfull[0], (h_issued - 1) & 1, p.err);
+      }
     }
   } else {
     // ------------------------------------------------------------ epilogue

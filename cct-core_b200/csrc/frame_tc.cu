@@ -15,8 +15,9 @@
 //              j copies, for every chunk q = j (mod 4), the pixel's split
 //              words of that tap into the chunk's tensor-memory stage
 //              (tcgen05.st, row m = lane m): four chunks are in flight.
-//   warp 16    MMA issuer: the warp probes the next 8 chunks at once and
-//              issues every ready one in a batch; one elected lane issues,
+//   warp 16    MMA issuer: for filters of kBatchTaps or more taps the warp
+//              probes the next 8 chunks at once and issues every ready one in
+//              a batch (else one chunk per wait); one elected lane issues,
 //              per 16-deep k-step of a chunk, with A from tensor memory and
 //              B from shared memory,
 //                A_hi x [B_hi; B_lo] (N = 2*NT) into [hh | small], then
@@ -32,7 +33,9 @@
 //              border) and bulk copies of the pre-packed filter chunks; the
 //              warp probes the next 8 stages at once and each lane issues the
 //              copy of one free stage, so a batch of copies goes out together
-//              (one thread looping over them issued one per ~480 cycles).
+//              (one thread looping over them issued one per ~480 cycles);
+//              for filters of fewer than kBatchTaps taps one thread issues one
+//              copy per loop trip.
 //   warps 18-25 epilogue, two per tensor-memory lane quarter taking
 //              alternate 16-column blocks: tcgen05.ld of the accumulator,
 //              optional ReLU, coalesced stores to the output planes.

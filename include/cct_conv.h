@@ -36,7 +36,7 @@ extern "C" {
 enum {
   CCT_OK = 0,
   CCT_EINVAL = -1,    /* descriptor rejected (same rules as the reference)   */
-  CCT_ENOTSUP = -2,   /* legal in the reference, not offered by this build   */
+  CCT_ENOTSUP = -2,   /* legal in the reference, not offered by this library */
   CCT_ENOMEM = -3,    /* device or host allocation failed                    */
   CCT_ECUDA = -4,     /* CUDA runtime / launch error                         */
   CCT_ETIMEOUT = -5,  /* a bounded device wait gave up                       */

@@ -44,6 +44,12 @@ void count_launches(uint64_t n) {
 }
 void set_launch_capture(bool on) { t_capturing = on; }
 
+// The device error word: one statically allocated word per device (module
+// data, zero at load), so neither a plan nor the allocation-free entry point
+// allocates it.  Its name is a host-side stand-in: the device address is
+// looked up once per device, with that device current, and cached for the
+// life of the CUDA context (cudaDeviceReset invalidates it).
+static __device__ unsigned g_dev_err_word;
 static std::mutex g_err_mu;
 static unsigned *g_err_word[64];
 
@@ -52,13 +58,9 @@ unsigned *device_error_word() {
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
   std::lock_guard<std::mutex> lk(g_err_mu);
   if (!g_err_word[dev]) {
-    unsigned *p = nullptr;
-    if (cudaMalloc(&p, sizeof(unsigned)) != cudaSuccess) return nullptr;
-    if (cudaMemset(p, 0, sizeof(unsigned)) != cudaSuccess) {
-      cudaFree(p);
-      return nullptr;
-    }
-    g_err_word[dev] = p;
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_dev_err_word) != cudaSuccess) return nullptr;
+    g_err_word[dev] = static_cast<unsigned *>(p);
   }
   return g_err_word[dev];
 }
@@ -332,7 +334,7 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
     algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
 
   unsigned *err_word = device_error_word();
-  if (!err_word) return set_error(CCT_ENOMEM, "device error word allocation failed");
+  if (!err_word) return set_error(CCT_ECUDA, "device error word: symbol address lookup failed");
 
   cct_conv_plan *p = new (std::nothrow) cct_conv_plan();
   if (!p) return set_error(CCT_ENOMEM, "plan allocation failed");
@@ -564,7 +566,8 @@ int cct_device_status(void) {
   int rc = check_cuda(cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost), "cudaMemcpy(status)");
   if (rc) return rc;
   if (v == 0) return CCT_OK;
-  cudaMemset(w, 0, sizeof(unsigned));
+  rc = check_cuda(cudaMemset(w, 0, sizeof(unsigned)), "cudaMemset(status)");
+  if (rc) return rc;
   return set_error(CCT_ETIMEOUT, "a bounded wait inside a kernel gave up (status 0x%x)", v);
 }
 

@@ -97,8 +97,9 @@ int launch_direct(const ConvGeom &g, const float *x, const float *f, float *y,
 bool direct_tma_supported(const ConvGeom &g, const float *x);
 int launch_direct_tma(const ConvGeom &g, const float *x, const float *f, float *y,
                       cudaStream_t stream, unsigned *err);
-// Per-device error word passed to kernels with bounded waits (allocated on
-// first use on the current device).
+// Per-device error word passed to kernels with bounded waits: a statically
+// allocated device word whose address is looked up on first use on the
+// current device (nothing is allocated).  nullptr if the lookup fails.
 unsigned *device_error_word();
 // FilterAdjoint with small results (fa_f32.cu): BorderValid, no sampling,
 // result width <= 8.  The block-reduced form needs fa_workspace_bytes() of

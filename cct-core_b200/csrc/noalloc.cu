@@ -10,8 +10,14 @@
 //  - latency-sensitive callers: cudaMalloc and cudaFree may synchronise the
 //    device and stall every stream, not just the caller's.
 // Those callers pass device pointers for the image, filter and output; the
-// only scratch, the packed bf16 hi/lo filter operand (and a small status
-// word), lives in the file-scope array below.
+// only scratch, the packed bf16 hi/lo filter operand, lives in the
+// file-scope array below.
+//
+// Failure reporting: the kernel's bounded waits record a timeout in the
+// library's device error word, which is itself a statically allocated device
+// word (nothing allocates it), the same word every plan's kernels use.  It
+// is not cleared per call: a timeout stays recorded until cct_device_status()
+// reads and clears it.
 //
 // Limits and sharing:
 //  - the packed filter operand must fit in kNoAllocScratchBytes (4 MiB);
@@ -19,10 +25,13 @@
 //  - every GPU that loads this library holds the array until the process
 //    exits;
 //  - all calls on a device share the array and it keeps the last call's
-//    contents: each call rewrites the whole packed operand it uses and
-//    clears the status word first, so nothing stale is read, but calls that
-//    overlap on the GPU (different streams, no ordering between them) race
-//    on it.
+//    contents: each call rewrites the whole packed operand it uses, so
+//    nothing stale is read, but calls that overlap on the GPU (different
+//    streams, no ordering between them) race on it;
+//  - the array's device address (and the error word's) is looked up on the
+//    first call on each device and cached for the life of the CUDA context:
+//    make that first call before any stream capture, and not across a
+//    cudaDeviceReset.
 #include <mutex>
 
 #include "cct_internal.h"
@@ -31,10 +40,8 @@
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = (size_t)4 << 20;  // packed filter operand limit
-constexpr size_t kStatusOffset = kNoAllocScratchBytes;     // status word after the operand
 
-// Packed filter operand [0, 4 MiB) + a 256-byte status region.
-static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes + 256];
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_noalloc_mu;
 uint8_t *g_noalloc_addr[64];  // device address of g_noalloc_scratch, per device
@@ -92,10 +99,9 @@ extern "C" int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *imag
   uint8_t *scratch = nullptr;
   rc = scratch_address(dev, &scratch);
   if (rc) return rc;
-  unsigned *status = reinterpret_cast<unsigned *>(scratch + kStatusOffset);
+  unsigned *status = device_error_word();
+  if (!status) return set_error(CCT_ECUDA, "device error word: symbol address lookup failed");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  rc = check_cuda(cudaMemsetAsync(status, 0, sizeof(unsigned), st), "cudaMemsetAsync(status)");
-  if (rc) return rc;
   rc = launch_pack_filters(tc, filter, scratch, st);
   if (rc) return rc;
   return launch_frame_tc(tc, image, out, scratch, status, st);

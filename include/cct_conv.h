@@ -213,9 +213,12 @@ int cct_color_plan_destroy(cct_color_plan *plan);
  * until exit).  Descriptors whose packed operand exceeds 4 MiB are rejected
  * with CCT_EINVAL; shapes the tensor-core kernel does not take return
  * CCT_ENOTSUP.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  All calls on a device share the array: calls that overlap on
- * the GPU race and must be ordered by the caller. */
+ * address (cudaGetSymbolAddress) and caches it for the life of the CUDA
+ * context; make that first call before any stream capture.  All calls on a
+ * device share the array: calls that overlap on the GPU race and must be
+ * ordered by the caller.  A bounded wait that gives up inside this kernel is
+ * recorded in the same statically allocated device error word as every
+ * plan's kernels, and reported (then cleared) by cct_device_status(). */
 int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *image,
                          const float *filter, float *out, void *stream);
 
@@ -373,7 +376,9 @@ int cct_stream_synchronize(void *stream);
  * gave up (that kernel returned early and its output is undefined).  The
  * reference surfaces device failures as a CLEvent error status
  * (src/main/scala/cogx/platform/opencl/OpenCLDeviceKernel.scala:106-147).
- * Reading clears the status; the call synchronises with the device. */
+ * Reading clears the status; the call synchronises with the device.  It
+ * covers plans, graphs, servers and cct_conv_run_noalloc alike: all of them
+ * record into one statically allocated word per device. */
 int cct_device_status(void);
 /* Failure-detection self-test (no counterpart in the reference): launches a
  * kernel whose mbarrier wait never completes, so the library's bounded wait

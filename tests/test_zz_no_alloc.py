@@ -109,3 +109,48 @@ def test_noalloc_result_matches_fp64_oracle():
     od = O.make_desc(H, W, R, R, planes=B * C, f_planes=K * C, batch=B, border=O.ZERO,
                      orient=O.XCORR, mode=O.PROJECT_REDUCE)
     assert O.rel_errors(y.cpu().numpy(), O.conv(od, x, f, np.float64))[0] <= TOL
+
+
+def _filter_bank_case():
+    B, C, K, H, W, R = 2, 16, 32, 24, 24, 3
+    desc = _desc(H, W, R, B * C, K * C, B, _lib.CROSS_CORRELATION, _lib.PROJECT_FRAME_BLOCK_REDUCE_SUM)
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.randn((B * C, H, W), device="cuda", generator=gen)
+    f = torch.randn((K * C, R, R), device="cuda", generator=gen)
+    return desc, x, f, (B * K, H, W)
+
+
+def test_noalloc_timeouts_are_reported_by_device_status():
+    """A bounded wait that gives up is recorded in the library's one device
+    error word, which this entry point's kernel shares with every plan; a
+    call does not clear it, and cct_device_status() reports and clears it."""
+    desc, x, f, oshape = _filter_bank_case()
+    y = torch.empty(oshape, device="cuda")
+    assert _run_noalloc(desc, x, f, y) == _lib.OK
+    torch.cuda.synchronize()
+    assert _lib.LIB.cct_device_status() == _lib.OK  # a clean run records nothing
+    # record a timeout in the word (a wait on a barrier nobody arrives on,
+    # which gives up after about a second and returns: no fault)
+    assert _lib.LIB.cct_selftest_wait_timeout(None) == _lib.OK
+    y2 = torch.empty(oshape, device="cuda")
+    assert _run_noalloc(desc, x, f, y2) == _lib.OK
+    torch.cuda.synchronize()
+    assert _lib.LIB.cct_device_status() == _lib.ETIMEOUT  # still recorded after the call
+    assert _lib.LIB.cct_device_status() == _lib.OK  # reading cleared it
+    assert torch.equal(y, y2)  # and the context still computes the same result
+
+
+def test_noalloc_allocates_no_device_memory():
+    """Free device memory is the same before and after 100 calls (after the
+    first, which loads the kernels and looks up the scratch address)."""
+    desc, x, f, oshape = _filter_bank_case()
+    y = torch.empty(oshape, device="cuda")
+    assert _run_noalloc(desc, x, f, y) == _lib.OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(100):
+        assert _run_noalloc(desc, x, f, y) == _lib.OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert _lib.LIB.cct_device_status() == _lib.OK

@@ -18,7 +18,7 @@ and ``src/test/scala/cogx/DynamicConvolutionSpec.scala:40-72``): Java
 big-endian float32 values with columns in the inner loop.
 
 Run (only where the reference tree is present):
-    python tests/golden/make_golden.py [reference_root]
+    python tests/golden/make_golden.py <reference_root>
 """
 import struct
 import sys
@@ -78,7 +78,9 @@ def read_hdr(path):
 
 
 def main():
-    root = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference_root>  (the cct-core source tree)")
+    root = Path(sys.argv[1])
     src = root / SUBDIR
     out = {}
     for i in range(25):

@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--workload", choices=["frame", "plain", "fft", "graph", "serve"], default="frame")
     ap.add_argument("--precision", choices=["auto", "fp32", "bf16x3"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-suite", action="store_true",
+                    help="headline workload only (no sub-results for the other workloads)")
     ap.add_argument("--serve-requests", type=int, default=10000)
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     return ap.parse_args()
@@ -150,6 +152,39 @@ class ClockSampler:
                           if v.lower() == "active"})
         return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": rows[0][1],
                 "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- configs
+# One config dict per workload, printed identically by the GPU arm and the
+# reference (CPU) arm, so both lines name the same workload.
+def frame_config():
+    return {"workload": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 "
+                        "K=64 64x64 5x5 BorderZero", "B": 16, "C": 32, "K": 64, "H": 64, "W": 64,
+            "R": 5, "border": "BorderZero", "l2": "6 rotating input/output sets (288 MB > 126 MB L2)"}
+
+
+def plain_config():
+    return {"workload": "plain convolve 256x256 (*) 5x5 BorderZero, 4096 planes per launch",
+            "planes": 4096, "H": 256, "W": 256, "R": 5, "l2": "1 GiB input > 126 MB L2"}
+
+
+def fft_config():
+    return {"workload": "FFT convolve 2048x2048 uniform[0,1] (*) 63x63 normalised Gaussian "
+                        "(sigma 10), BorderCyclic, static filter",
+            "H": 2048, "W": 2048, "R": 63, "border": "BorderCyclic",
+            "flops": "direct-equivalent 2*H*W*R*S per convolution",
+            "l2": "8 rotating image/output sets (268 MB > 126 MB L2)"}
+
+
+def graph_config(batch=64):
+    return {"workload": "eight-layer 3x3 stack on 224x224x3 (widths 64,64,128,128,256,256,512,512; "
+                        "DownsampleOutput(2) after layers 2,4,6; ReLU between layers), "
+                        f"batch {batch}, one CUDA-graph replay per step",
+            "batch": batch, "layers": 8, "gflop_per_step": round(12.196 * batch, 2),
+            "l2": "activations of batch 64 (1.2 GB per step) exceed the 126 MB L2"}
+
+
+CONFIGS = {"frame": frame_config, "plain": plain_config, "fft": fft_config, "graph": graph_config}
 
 
 # ----------------------------------------------------------------------------- workloads
@@ -300,9 +335,7 @@ def frame_workload(precision):
         "gflop_per_step": 2 * GFLOP_FRAME, "gflop_per_launch": GFLOP_FRAME,
         "h2d": nbytes(hx) + nbytes(hg) + nbytes(hf), "d2h": nbytes(hy) + nbytes(hdx),
         "metric": "GFLOP/s", "unit": "GFLOP/s", "precision": precision, "plan_algo": fwd.algo,
-        "config": {"workload": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 "
-                               "K=64 64x64 5x5 BorderZero", "B": B, "C": Cin, "K": K, "H": H, "W": W,
-                   "R": R, "border": "BorderZero", "l2": "6 rotating input/output sets (288 MB > 126 MB L2)"},
+        "config": frame_config(),
         "dtype": "f32" if precision == "fp32" else "bf16x3 split, f32 accumulate",
         "keep": (fwd, bwd, xs, gs, ys, dxs, f, hx, hg, hf, hy, hdx),
         # evaluated after the timed region, so the step launches come first in a launch list
@@ -399,8 +432,7 @@ def plain_workload():
         "bytes_per_step": byts, "e2e_gb_per_step": 4 * (2 * 64 * H * W + R * R) / 1e9,
         "h2d": 4 * (64 * H * W + R * R), "d2h": 4 * 64 * H * W,
         "metric": "GB/s", "unit": "GB/s", "precision": "fp32", "plan_algo": plan.algo,
-        "config": {"workload": "plain convolve 256x256 (*) 5x5 BorderZero, 4096 planes per launch",
-                   "planes": P, "H": H, "W": W, "R": R, "l2": "1 GiB input > 126 MB L2"},
+        "config": plain_config(),
         "dtype": "f32", "keep": (plan, plan64, one, x, y, f, hx, hy, hf, rf, cf, tmp),
         "kernel": "direct_tma_kernel", "bytes_per_launch": byts,
     }
@@ -485,11 +517,7 @@ def fft_workload():
         "bytes_per_launch": 4 * n * n * 2 + 8 * n * (n // 2 + 1),
         "e2e_gb_per_step": None, "h2d": 4 * n * n, "d2h": 4 * n * n,
         "metric": "GFLOP/s", "unit": "GFLOP/s", "precision": "fp32", "plan_algo": plan.algo,
-        "config": {"workload": "FFT convolve 2048x2048 uniform[0,1] (*) 63x63 normalised Gaussian "
-                               "(sigma 10), BorderCyclic, static filter",
-                   "H": n, "W": n, "R": k, "border": "BorderCyclic",
-                   "flops": "direct-equivalent 2*H*W*R*S per convolution",
-                   "l2": "8 rotating image/output sets (268 MB > 126 MB L2)"},
+        "config": fft_config(),
         "dtype": "f32", "keep": (plan, direct, dyn, xs, ys, fd, yd, hx, hy),
         "kernel": "fft_rows_r2c+fft_cols+fft_rows_c2r", "fft_hbm_roofline": True,
         "extra": {"error_vs_fp64": err, "direct_ms": round(direct_s * 1e3, 4),
@@ -601,11 +629,7 @@ def graph_workload(precision):
         "h2d": hx.numel() * 4, "d2h": hy.numel() * 4,
         "metric": "GFLOP/s", "unit": "GFLOP/s", "precision": "fp32" if prec == _lib.PREC_FP32 else "bf16x3",
         "plan_algo": last.algo,
-        "config": {"workload": "eight-layer 3x3 stack on 224x224x3 (widths 64,64,128,128,256,256,512,512; "
-                               "DownsampleOutput(2) after layers 2,4,6; ReLU between layers), "
-                               f"batch {B}, one CUDA-graph replay per step",
-                   "batch": B, "layers": 8, "gflop_per_step": round(gflop, 2),
-                   "l2": "activations of batch 64 (1.2 GB per step) exceed the 126 MB L2"},
+        "config": graph_config(B),
         "dtype": "f32" if prec == _lib.PREC_FP32 else "bf16x3 split, f32 accumulate",
         "keep": (stack, last, lin, lf, ly, hx, hy),
         "kernel": "frame_tc_kernel (layer 8)" if prec != _lib.PREC_FP32 else "frame_f32_kernel (layer 8)",
@@ -625,32 +649,32 @@ def serve_requests(n, seed=5):
     return [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(side, R, C, K)]
 
 
-def run_serve(args):
-    """Continuous batching vs plain per-call dispatch on the same request
-    stream (rank 0 only; every rank serves its own stream under torchrun)."""
-    import numpy as np
-    import torch
-    from cctconv import _lib
-    from cctconv.serve import Server, conv_request
+class ServeBench:
+    """Continuous batching vs plain per-call dispatch on one seeded request
+    stream: a shared pinned input pool (requests read its start), a ring of
+    pinned output space, resident filter banks per (R, C, K)."""
 
-    rank, world, local, pg = dist_setup(args.gpus)
-    rng = np.random.default_rng(5)
-    specs = serve_requests(args.serve_requests)
-    max_in = max(s * s * c for s, r, c, k in specs)
-    max_out = max(s * s * (c if k == 1 else k) for s, r, c, k in specs)
-    # one shared input pool (requests read its start) and a ring of output space
-    pool = torch.from_numpy(rng.uniform(-1, 1, max_in).astype(np.float32)).pin_memory()
-    ring_elems = max(4 * max_out, 1 << 29)
-    ring = torch.empty(ring_elems).pin_memory()
+    def __init__(self, n_requests):
+        import numpy as np
+        import torch
+        self.rng = np.random.default_rng(5)
+        self.specs = serve_requests(n_requests)
+        max_in = max(s * s * c for s, r, c, k in self.specs)
+        max_out = max(s * s * (c if k == 1 else k) for s, r, c, k in self.specs)
+        self.pool = torch.from_numpy(self.rng.uniform(-1, 1, max_in).astype(np.float32)).pin_memory()
+        self.ring_elems = max(4 * max_out, 1 << 29)
+        self.ring = torch.empty(self.ring_elems).pin_memory()
 
-    def build(server):
+    def build(self, server):
+        from cctconv import _lib
+        from cctconv.serve import conv_request
         banks, reqs, flops, hbytes = {}, [], 0.0, 0
         pos = 0
-        for side, R, C, K in specs:
+        for side, R, C, K in self.specs:
             key = (R, C, K)
             if key not in banks:
                 fp = 1 if K == 1 else K * C
-                banks[key] = server.add_filter(rng.uniform(-1, 1, (fp, R, R)).astype(np.float32))
+                banks[key] = server.add_filter(self.rng.uniform(-1, 1, (fp, R, R)).astype("float32"))
             if K == 1:
                 d = _lib.new_desc(image_rows=side, image_cols=side, image_planes=C if C > 1 else 0,
                                   filter_rows=R, filter_cols=R, filter_planes=0,
@@ -662,17 +686,19 @@ def run_serve(args):
                                   vector_mode=_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM)
                 planes = K
             out = side * side * planes
-            if pos + out > ring_elems:
+            if pos + out > self.ring_elems:
                 pos = 0
-            reqs.append(conv_request(d, pool.data_ptr(), ring.data_ptr() + 4 * pos, None, banks[key]))
+            reqs.append(conv_request(d, self.pool.data_ptr(), self.ring.data_ptr() + 4 * pos, None, banks[key]))
             pos += (out + 63) // 64 * 64
             flops += 2.0 * side * side * planes * R * R * (C if K > 1 else 1)
             hbytes += 4 * side * side * (C + planes)
         return reqs, flops, hbytes
 
-    def run(per_call, rate, n):
+    def run(self, per_call, rate, n):
+        import numpy as np
+        from cctconv.serve import Server
         server = Server(slots=4, max_batch=64, arena_bytes=16 << 30, per_call=per_call)
-        reqs, flops, hbytes = build(server)
+        reqs, flops, hbytes = self.build(server)
         reqs, k = reqs[:n], n / len(reqs)
         arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))
         t0 = time.perf_counter()
@@ -686,12 +712,36 @@ def run_serve(args):
                 "GFLOP/s": round(flops * k / wall / 1e9, 1), "host_GB/s": round(hbytes * k / wall / 1e9, 2),
                 "batches": st["batches"], "solo": st["solo"]}
 
-    head = run(False, args.serve_rate, args.serve_requests)
-    base = run(True, args.serve_rate, min(args.serve_requests, 3000))
+
+SERVE_CONFIG = ("Poisson arrivals, side log-uniform 32-1024, R {3,5,7,9}, planes {1,4,16,64}, "
+                "filters {1,16,64}, FP32 host I/O, resident filter banks")
+
+
+def serve_suite(args, rates=(1000.0, 5000.0), n=2000):
+    """The serving loop beside the headline: batched and per-call dispatch at
+    two arrival rates on the first n requests of the seeded stream, with the
+    clocks sampled while they run."""
+    import torch
+    sb = ServeBench(n)
+    out = {"config": {"workload": f"{n} requests per rate, " + SERVE_CONFIG}, "rates": []}
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        for rate in rates:
+            out["rates"].append({"batched": sb.run(False, rate, n), "per_call": sb.run(True, rate, n)})
+    out["clocks"] = clocks.summary()
+    return out
+
+
+def run_serve(args):
+    """Continuous batching vs plain per-call dispatch on the same request
+    stream (rank 0 only; every rank serves its own stream under torchrun)."""
+    rank, world, local, pg = dist_setup(args.gpus)
+    sb = ServeBench(args.serve_requests)
+    head = sb.run(False, args.serve_rate, args.serve_requests)
+    base = sb.run(True, args.serve_rate, min(args.serve_requests, 3000))
     sweep = []
     for rate in (1000.0, 2000.0, 5000.0, 10000.0, 20000.0, 50000.0):
         n = min(args.serve_requests, 1500)
-        sweep.append({"batched": run(False, rate, n), "per_call": run(True, rate, n)})
+        sweep.append({"batched": sb.run(False, rate, n), "per_call": sb.run(True, rate, n)})
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
@@ -701,9 +751,7 @@ def run_serve(args):
         "n_gpus": world, "steps": args.serve_requests, "warmup": 0,
         "ms_per_step": round(1e3 / head["served_per_s"], 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.serve_requests} requests, Poisson arrivals at {args.serve_rate:g}/s, "
-                               "side log-uniform 32-1024, R {3,5,7,9}, planes {1,4,16,64}, "
-                               "filters {1,16,64}, FP32 host I/O, resident filter banks",
+        "config": {"workload": f"{args.serve_requests} requests at {args.serve_rate:g}/s, " + SERVE_CONFIG,
                    "parallelism": f"replicas{world}"},
         "latency": {"p50_ms": head["p50_ms"], "p99_ms": head["p99_ms"]},
         "per_call": base, "batched": head, "sweep": sweep,
@@ -908,13 +956,8 @@ def run_reference(args):
     value = statistics.median(per)
     sample = f"median of {samples} samples, last: {sample}"
     unit = "GB/s" if args.workload == "plain" else "GFLOP/s"
-    cfg = {"workload": {
-        "frame": "projectFrame+backProjectFrame (BlockReduceSum fused), B=16 C=32 K=64 64x64 5x5 "
-                 "BorderZero",
-        "plain": "plain convolve 256x256 (*) 5x5 BorderZero",
-        "fft": "convolve 2048x2048 (*) 63x63 normalised Gaussian (sigma 10), BorderCyclic "
-               "(direct-equivalent flops)",
-        "graph": "eight-layer 3x3 stack on 224x224x3, one layer-8 sample (28x28, 512->512)"}[args.workload]}
+    # the same config dict as the GPU arm's line for this workload
+    cfg = dict(CONFIGS[args.workload](), parallelism=f"replicas{args.gpus}")
     line = {"impl": "reference", "metric": unit, "value": round(value, 3), "unit": unit,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -929,38 +972,29 @@ def run_reference(args):
     return 0
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    if args.workload == "serve":
-        return run_serve(args)
+def measure(wl, steps, warmup, pg, world, peaks, peak_kind):
+    """Device-timed value, dominant-kernel roofline, end-to-end rate and
+    clocks of one workload: W untimed steps, K timed steps between CUDA
+    events (max over ranks), the dominant kernel timed alone, then the same
+    step through the C-ABI with host buffers (copies inside the timed
+    region)."""
     import torch
-    from cctconv import _lib
-
-    rank, world, local, pg = dist_setup(args.gpus)
-    wl = {"frame": lambda: frame_workload(args.precision), "plain": plain_workload,
-          "fft": fft_workload, "graph": lambda: graph_workload(args.precision)}[args.workload]()
-    peaks, peak_kind = load_peaks()
-
     with ClockSampler(torch.cuda.current_device()) as clocks:
-        elapsed, launches = time_steps(wl["step"], args.steps, args.warmup, pg)
+        elapsed, launches = time_steps(wl["step"], steps, warmup, pg)
     t_max = max_over_ranks(pg, elapsed)
-
     per_launch = time_single_launch(wl["launch_single"])
-    e2e_t, _ = time_steps(wl["e2e_step"], max(args.steps // 20, 3), 2, pg, wl.get("e2e_begin"),
-                          wl.get("e2e_finish"))
+    e2e_steps = max(steps // 20, 3)
+    e2e_t, _ = time_steps(wl["e2e_step"], e2e_steps, 2, pg, wl.get("e2e_begin"), wl.get("e2e_finish"))
     e2e_t = max_over_ranks(pg, e2e_t)
-    e2e_steps = max(args.steps // 20, 3)
 
     if wl.get("fft_hbm_roofline"):
         # FFT: reported in direct-equivalent GFLOP/s; its roofline is HBM
-        value = replica_value(wl["gflop_per_step"] * args.steps, world, t_max)
+        value = replica_value(wl["gflop_per_step"] * steps, world, t_max)
         e2e_val = replica_value(wl["gflop_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["bytes_per_launch"] / per_launch / 1e9
         bound, peak, unit = "hbm", peaks["hbm_gbs"], "GB/s"
     elif wl["unit"] == "GFLOP/s":
-        value = replica_value(wl["gflop_per_step"] * args.steps, world, t_max)
+        value = replica_value(wl["gflop_per_step"] * steps, world, t_max)
         e2e_val = replica_value(wl["gflop_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["gflop_per_launch"] / per_launch / 1e3  # TFLOP/s
         if wl["precision"] == "bf16x3":
@@ -970,10 +1004,77 @@ def main():
             bound, unit = "fp32_simt", "TFLOP/s"
             peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) / 1e6
     else:
-        value = replica_value(wl["bytes_per_step"] * args.steps, world, t_max) / 1e9
+        value = replica_value(wl["bytes_per_step"] * steps, world, t_max) / 1e9
         e2e_val = replica_value(wl["e2e_gb_per_step"] * e2e_steps, world, e2e_t)
         achieved = wl["bytes_per_launch"] / per_launch / 1e9
         bound, peak, unit = "hbm", peaks["hbm_gbs"], "GB/s"
+    return {
+        "metric": wl["metric"], "value": round(value, 3), "unit": wl["unit"],
+        "steps": steps, "warmup": warmup, "ms_per_step": round(1e3 * t_max / steps, 4),
+        "dtype": wl["dtype"], "config": dict(wl["config"], parallelism=f"replicas{world}"),
+        "roofline": {"bound": bound, "achieved": round(achieved, 3), "peak": round(peak, 1),
+                     "unit": unit, "frac": round(achieved / peak, 4), "traffic": load_traffic(wl["kernel"]),
+                     "peak_source": peak_kind if bound != "fp32_simt" else "nominal FP32 at sm_max_mhz",
+                     "kernel": wl["kernel"], "launch_ms": round(per_launch * 1e3, 4)},
+        "e2e": {"value": round(e2e_val, 3), "unit": wl["unit"], "h2d_bytes_per_step": wl["h2d"],
+                "d2h_bytes_per_step": wl["d2h"]},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "plan_algo": wl["plan_algo"],
+    }
+
+
+def sub_result(build, steps, warmup, pg, world, peaks, peak_kind):
+    """One workload measured beside the headline, with its extras (errors
+    against FP64, neighbouring operators); its device memory is released
+    before the next one."""
+    import gc
+    import torch
+    wl = build()
+    out = measure(wl, steps, warmup, pg, world, peaks, peak_kind)
+    extra = wl.get("extra", {})
+    out.update(extra() if callable(extra) else extra)
+    del wl
+    gc.collect()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.workload == "serve":
+        return run_serve(args)
+    import torch
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    wl = {"frame": lambda: frame_workload(args.precision), "plain": plain_workload,
+          "fft": fft_workload, "graph": lambda: graph_workload(args.precision)}[args.workload]()
+    peaks, peak_kind = load_peaks()
+    head = measure(wl, args.steps, args.warmup, pg, world, peaks, peak_kind)
+
+    extra = wl.get("extra", {})
+    extra = extra() if callable(extra) else extra
+    suite = {}
+    if args.workload == "frame" and world == 1 and not args.no_suite:
+        # Every other workload, driver-timed in the same run (one GPU): the
+        # plain FP32 filter bank on the same step (the denominator of the
+        # split-BF16 speed-up), the memory-bound plane convolution, the FFT
+        # path, the eight-layer stack and the serving loop.
+        del wl
+        sub_steps, sub_warm = max(args.steps, 10), max(args.warmup, 3)
+        fp32 = sub_result(lambda: frame_workload("fp32"), sub_steps, sub_warm, pg, world, peaks, peak_kind)
+        fp32.pop("weight_gradient_5x5", None)
+        suite["frame_fp32"] = fp32
+        if head["dtype"] != fp32["dtype"]:
+            suite["frame_fp32"]["split_bf16_speedup"] = round(head["value"] / fp32["value"], 3)
+        suite["plain_convolve"] = sub_result(plain_workload, sub_steps, sub_warm, pg, world, peaks, peak_kind)
+        suite["fft_convolve"] = sub_result(fft_workload, sub_steps, sub_warm, pg, world, peaks, peak_kind)
+        suite["graph_stack"] = sub_result(lambda: graph_workload(args.precision), max(args.steps // 2, 5),
+                                          sub_warm, pg, world, peaks, peak_kind)
+        suite["serving"] = serve_suite(args)
 
     if rank != 0:
         if pg is not None:
@@ -984,27 +1085,18 @@ def main():
         fn = {"frame": cpu_frame_sample, "plain": cpu_plain_sample,
               "fft": cpu_fft_sample, "graph": cpu_graph_sample}[args.workload]
         v, threads, sample = fn(seconds_budget=10.0)
-        cpu = {"value": round(v, 3), "unit": wl["unit"], "cores": threads, "kind": "port",
+        cpu = {"value": round(v, 3), "unit": head["unit"], "cores": threads, "kind": "port",
                "sample": sample}
-    traffic = load_traffic(wl["kernel"])
     line = {
-        "metric": wl["metric"], "value": round(value, 3), "unit": wl["unit"], "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_max / args.steps, 4),
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
-        "data": "synthetic (seeded)", "config": dict(wl["config"], parallelism=f"replicas{world}"),
-        "roofline": {"bound": bound, "achieved": round(achieved, 3), "peak": round(peak, 1),
-                     "unit": unit, "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_source": peak_kind if bound != "fp32_simt" else "nominal FP32 at sm_max_mhz",
-                     "kernel": wl["kernel"], "launch_ms": round(per_launch * 1e3, 4)},
-        "cpu_baseline": cpu,
-        "e2e": {"value": round(e2e_val, 3), "unit": wl["unit"], "h2d_bytes_per_step": wl["h2d"],
-                "d2h_bytes_per_step": wl["d2h"]},
-        "gpu_launches": int(launches),
-        "clocks": clocks.summary(),
-        "plan_algo": wl["plan_algo"],
+        "metric": head["metric"], "value": head["value"], "unit": head["unit"], "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": head["dtype"],
+        "data": "synthetic (seeded)", "config": head["config"],
+        "roofline": head["roofline"], "cpu_baseline": cpu, "e2e": head["e2e"],
+        "gpu_launches": head["gpu_launches"], "clocks": head["clocks"], "plan_algo": head["plan_algo"],
     }
-    extra = wl.get("extra", {})
-    line.update(extra() if callable(extra) else extra)
+    line.update(extra)
+    line.update(suite)
     print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

@@ -19,7 +19,7 @@ CROSS_CORRELATION, CONVOLUTION = 0, 1
 SAMPLE_NONE, SAMPLE_DOWN, SAMPLE_UP = 0, 1, 2
 (PLANE_BY_PLANE, PROJECT_FRAME, PROJECT_FRAME_BLOCK_REDUCE_SUM, BACK_PROJECT_FRAME,
  BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM, FILTER_ADJOINT, FILTER_ADJOINT_BLOCK_REDUCE_SUM) = range(7)
-PREC_FP32, PREC_BF16X3 = 0, 1
+PREC_FP32, PREC_BF16X3, PREC_BF16X6 = 0, 1, 2
 ALGO_AUTO, ALGO_DIRECT, ALGO_FFT = 0, 1, 2
 FLAG_RELU = 0x1
 PLAN_DIRECT, PLAN_FRAME_F32, PLAN_FRAME_BF16X3, PLAN_FFT, PLAN_FILTER_ADJOINT, PLAN_FILTER_ADJOINT_BF16X3 = range(6)

@@ -1,0 +1,771 @@
+// Fused filter-bank convolution on the tcgen05 tensor cores, split BF16:
+// ProjectFrameBlockReduceSum / BackProjectFrameBlockReduceSum
+// (ConvolveHyperKernel.scala:153-199, 319-340, 574-645), every border policy
+// (:235-317), DownsampleOutput(1, 2) (:205-223), any field width.
+//
+// GEMM view, per image b and block of 64 filters:
+//   D[filter k][position p] = sum over (plane c, tap t) F[k][c, t] * X[c][p + off(t)]
+// M = the filter block, N = a tile of output positions, reduction = planes x
+// taps.  Positions live on a padded output grid of pitch P = BW + (S-1)/step
+// columns (a band of BW output columns plus the tap reach): the input value a
+// position reads at tap t then sits at a fixed offset off(t) from the
+// position on the same grid, so the B operand of tap t is a contiguous run of
+// the halo in shared memory and the tensor core reads it through a shifted
+// descriptor -- no per-tap copies.  Grid columns past the band's outputs are
+// computed and discarded ((S-1)/P of the work).  DownsampleOutput(2) holds
+// the input as its four polyphase components, each a stride-1 grid.
+//
+// Split precision.  x = xh + xl (+ xm) and f likewise, each term bf16.  The
+// filter operand of one MMA is 128 rows: rows 0-63 ("big") multiply into the
+// hi*hi sum only, rows 64-127 ("small") into the correction products:
+//   2 terms (BF16X3): [Fh; Fl] x Xh  and  [0; Fh] x Xl
+//                     -> big hh, small lh + hl
+//   3 terms (BF16X6): [Fh; Fm] x Xh, [0; Fh] x Xm, [0; Fh] x Xl, [0; Fl] x Xh,
+//                     [0; Fm] x Xm
+//                     -> big hh, small mh + hm + hl + lh + mm
+// The big rows never receive a small addend: the tensor core's FP32
+// accumulation drops the bits of an addend below the accumulator's last
+// place, and measured that way its error grows with the number of MMAs
+// accumulated, so only hh goes into the big sum and zero rows (which add
+// exactly 0) fill the big half of the other MMAs.  For long reductions the
+// accumulator is also promoted: every seg_stages stages the epilogue adds it
+// into an FP32 running sum (RN, CUDA cores) and the next MMA starts it
+// afresh, which bounds the accumulation error by the segment length.  The
+// epilogue adds each filter's big and small rows.
+//
+// Warp roles (one persistent CTA per SM, 576 threads):
+//   warps 0-7   converters: for each (tile, plane block) fill a halo buffer:
+//               plain loads of the input with the border policy applied
+//               (zero, clamp, cyclic), split into bf16 terms, stored in the
+//               K-major core-matrix layout [plane group][position][8 planes];
+//               two buffers, so the next block is converted while the
+//               current one is multiplied.
+//   warp 8      MMA issuer (one elected lane): per (tile, plane block, tap):
+//               KS k-steps x nmma MMAs, A = filter chunk stage, B = halo.
+//   warp 9      loader (one lane): bulk copies of the pre-packed filter
+//               chunks (nb, plane block, tap) into a ring of stages.
+//   warps 10-17 epilogue, two per tensor-memory lane quarter (alternate
+//               column halves): promotion adds, then the big + small
+//               combination (small rows pass through shared memory to the
+//               warp holding the same filters' big rows), ReLU, stores.
+// Every wait is bounded: on a timeout the CTA records it in the device error
+// word, lets its copies and MMAs land, frees tensor memory and exits.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <unordered_map>
+
+#include "bank_tc.h"
+#include "sm100_util.cuh"
+
+namespace cct {
+namespace {
+
+constexpr int kConvWarps = 8;
+constexpr int kConvThreads = 32 * kConvWarps;
+constexpr int kMmaWarp = kConvWarps;
+constexpr int kLoadWarp = kConvWarps + 1;
+constexpr int kEpiWarp0 = kConvWarps + 2;
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
+constexpr int kMaxStages = 8;
+constexpr uint32_t kAccCols = 256;  // one accumulator (N <= 256 fp32 columns)
+// Epilogue exchange: per warp pair two buffers of 32 filters x 16 positions
+// (row pitch 17 floats: conflict-free by filter and by position).
+constexpr int kXchPitch = 17;
+constexpr int kXchFloats = 32 * kXchPitch;
+constexpr size_t kXchBytes = 4 * 2 * kXchFloats * sizeof(float);
+
+// Filter chunk row blocks (64 rows each) and the MMAs over them.
+// Block contents: -1 zero, else the split term (0 hi, 1 mid / lo for 2 terms, 2 lo).
+__host__ __device__ constexpr int block_term(int terms, int blk) {
+  return terms == 2 ? (blk == 0 ? -1 : blk - 1)                          // Z Fh Fl
+                    : (blk == 0 || blk == 3 || blk == 5 ? -1             // Z Fh Fm Z Fl Z Fm
+                                                        : (blk == 1 ? 0 : blk == 2 ? 1 : blk == 4 ? 2 : 1));
+}
+template <int TERMS>
+struct MmaList;
+template <>
+struct MmaList<2> {
+  static constexpr int n = 2;
+  __device__ static int arow(int m) { return m == 0 ? 64 : 0; }  // [Fh; Fl], [0; Fh]
+  __device__ static int bterm(int m) { return m; }               // Xh, Xl
+};
+template <>
+struct MmaList<3> {
+  static constexpr int n = 5;
+  // [Fh; Fm] x Xh, [0; Fh] x Xm, [0; Fh] x Xl, [0; Fl] x Xh, [0; Fm] x Xm
+  __device__ static int arow(int m) { return m == 0 ? 64 : m == 3 ? 192 : m == 4 ? 320 : 0; }
+  __device__ static int bterm(int m) { return m == 0 || m == 3 ? 0 : m == 2 ? 2 : 1; }
+};
+
+struct Bars {
+  uint64_t full[kMaxStages], empty[kMaxStages];  // filter chunk stages
+  uint64_t hfull[2], hempty[2];                  // halo buffers
+  uint64_t dfull[2], dempty[2];                  // accumulators (one per segment in flight)
+  uint64_t drain;                                // MMA warp: every MMA retired
+  uint32_t tmem_slot;
+  int abort_flag;
+};
+
+// Border policy of the input (ConvolveHyperKernel.scala:235-317): maps
+// (iy, ix) into the field, or returns false for a zero.
+__device__ __forceinline__ bool border_map(const ConvGeom &g, int iy, int ix, int &ry, int &rx) {
+  if (g.border == CCT_BORDER_CLAMP) {
+    ry = min(max(iy, 0), g.H - 1);
+    rx = min(max(ix, 0), g.W - 1);
+    return true;
+  }
+  if (g.border == CCT_BORDER_CYCLIC) {
+    ry = ((iy % g.H) + g.H) % g.H;
+    rx = ((ix % g.W) + g.W) % g.W;
+    return true;
+  }
+  ry = iy;
+  rx = ix;
+  return iy >= 0 && iy < g.H && ix >= 0 && ix < g.W;
+}
+
+struct Item {
+  int b, band, tile, nb;
+};
+__device__ __forceinline__ Item decode(const BankParams &p, int i) {
+  Item it;
+  it.nb = i % p.nblocks;
+  int rest = i / p.nblocks;
+  it.tile = rest % p.tiles_band;
+  rest /= p.tiles_band;
+  it.band = rest % p.nbands;
+  it.b = rest / p.nbands;
+  return it;
+}
+
+// Split 8*KG planes of one halo position into bf16 terms and store them as
+// KG core-matrix rows (16 bytes per term).  src points at the position in
+// the first plane; `cvalid` planes exist (the rest are zero).  All 8*KG loads
+// are issued before the first store, so a converter thread keeps that many
+// reads in flight.
+template <int TERMS, int KG>
+__device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, bool in, int cvalid,
+                                                uint8_t *dst, uint32_t kg_stride, uint32_t part_bytes) {
+  float v[8 * KG];
+#pragma unroll
+  for (int j = 0; j < 8 * KG; ++j) v[j] = (in && j < cvalid) ? __ldg(src + j * plane) : 0.0f;
+#pragma unroll
+  for (int k = 0; k < KG; ++k) {
+    uint8_t *d = dst + k * kg_stride;
+    const float *w = v + 8 * k;
+    if (TERMS == 2) {
+      uint32_t hi[4], lo[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) split_bf16x2(w[2 * j], w[2 * j + 1], hi[j], lo[j]);
+      *reinterpret_cast<uint4 *>(d) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4 *>(d + part_bytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    } else {
+      uint32_t hi[4], mi[4], lo[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) split3_bf16x2(w[2 * j], w[2 * j + 1], hi[j], mi[j], lo[j]);
+      *reinterpret_cast<uint4 *>(d) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+      *reinterpret_cast<uint4 *>(d + part_bytes) = make_uint4(mi[0], mi[1], mi[2], mi[3]);
+      *reinterpret_cast<uint4 *>(d + 2 * (size_t)part_bytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+    }
+  }
+}
+
+template <int TERMS>
+__global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_constant__ BankParams p) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ Bars bars;
+  __shared__ float xch[4 * 2 * kXchFloats];  // epilogue exchange: 4 warp pairs x 2 buffers
+  const ConvGeom &g = p.g;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *halo = smem;                                 // 2 x halo_bytes
+  uint8_t *stage = smem + 2 * (size_t)p.halo_bytes;     // stages x stage_bytes
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.stages; ++s) {
+      mbar_init(&bars.full[s], 1);   // loader expect_tx
+      mbar_init(&bars.empty[s], 1);  // MMA commit
+    }
+    for (int h = 0; h < 2; ++h) {
+      mbar_init(&bars.hfull[h], kConvWarps);  // one arrival per converter warp
+      mbar_init(&bars.hempty[h], 1);          // MMA commit
+      mbar_init(&bars.dfull[h], 1);           // MMA commit
+      mbar_init(&bars.dempty[h], kEpiWarps);  // one arrival per epilogue warp
+    }
+    mbar_init(&bars.drain, 1);
+    bars.abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == kMmaWarp) tmem_alloc(&bars.tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = bars.tmem_slot;
+  // Nothing above touches global memory, so it may overlap the previous
+  // kernel in the stream (programmatic serialisation).
+  grid_dependency_wait();
+  allow_dependent_launch();
+
+  volatile int *abort_flag = &bars.abort_flag;
+  const int tstages = p.NCB * p.nst;                            // stages per tile
+  const int nseg = (tstages + p.seg_stages - 1) / p.seg_stages;  // accumulation segments per tile
+
+  if (warp < kConvWarps) {
+    // ------------------------------------------------------------ converters
+    const int nkg = p.CB / 8;                   // 2, 4 or 8 core-matrix columns
+    const uint32_t kgs = (uint32_t)p.L * 16;     // bytes between them
+    const size_t plane = (size_t)g.H * g.W;
+    uint32_t hb = 0;
+    bool failed = false;
+    for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
+      const Item it = decode(p, i);
+      const int p0 = it.tile * p.N;
+      const int col0 = it.band * p.BW + p.sc_min;  // strided input column of halo column 0
+      const float *xb = p.x + (size_t)it.b * g.n * plane;
+      for (int cb = 0; cb < p.NCB; ++cb, ++hb) {
+        const int buf = hb & 1;
+        if (*abort_flag || !mbar_wait(&bars.hempty[buf], ((hb >> 1) & 1) ^ 1, p.err)) {
+          failed = true;
+          break;
+        }
+        uint8_t *hbase = halo + (size_t)buf * p.halo_bytes;
+        const int cv = g.n - cb * p.CB;  // planes of this block that exist
+        const float *xc = xb + (size_t)cb * p.CB * plane;
+        for (int ph = 0; ph < p.nphase; ++ph) {
+          uint8_t *hph = hbase + (size_t)ph * TERMS * p.part_bytes;
+          for (int q = threadIdx.x; q < p.L; q += kConvThreads) {
+            const int G = p0 + q;
+            const int Y = G / p.P, X = G - Y * p.P;
+            const int iy = g.down * (Y + p.sr_min) + p.phase_r[ph];
+            const int ix = g.down * (col0 + X) + p.phase_c[ph];
+            int ry, rx;
+            const bool in = border_map(g, iy, ix, ry, rx);
+            const float *src = in ? xc + (size_t)ry * g.W + rx : xc;
+            uint8_t *dst = hph + (size_t)q * 16;
+            int kg = 0;
+            for (; kg + 4 <= nkg; kg += 4)
+              convert_kgroups<TERMS, 4>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
+                                        kgs, p.part_bytes);
+            for (; kg < nkg; kg += 2)
+              convert_kgroups<TERMS, 2>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
+                                        kgs, p.part_bytes);
+          }
+        }
+        // the tensor core reads the halo through the async proxy
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&bars.hfull[buf]);
+      }
+    }
+    if (failed) *abort_flag = 1;
+  } else if (warp == kMmaWarp) {
+    // ------------------------------------------------------------ MMA issuer
+    using ML = MmaList<TERMS>;
+    const uint32_t idesc = idesc_bf16_f32(128, p.N);
+    // Operand descriptors are a template (layout, strides) plus the address
+    // in 16-byte units; shared-memory addresses stay below 256 KB, so the
+    // address field never carries into the stride fields.
+    const uint64_t a_tmpl = smem_desc_kmajor(0, 128, (uint32_t)p.CB * 16);
+    const uint64_t b_tmpl = smem_desc_kmajor(0, (uint32_t)p.L * 16, 128);
+    const uint32_t stage0 = smem_u32(stage) >> 4, halo0 = smem_u32(halo) >> 4;
+    const uint32_t chunk16 = p.chunk_bytes >> 4, part16 = p.part_bytes >> 4, stage16 = p.stage_bytes >> 4;
+    const uint32_t kstep_b16 = 2u * p.L;              // B: two plane groups of L positions
+    const uint32_t row16 = (uint32_t)p.CB / 8;        // A: one filter row (CB bf16) in 16-byte units
+    uint32_t q = 0, hb = 0, u = 0;
+    bool failed = false;
+    for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
+      int seg_left = 0, done = 0, bi = 0;
+      bool first = false;
+      for (int cb = 0; cb < p.NCB && !failed; ++cb, ++hb) {
+        const int buf = hb & 1;
+        failed = __any_sync(0xffffffffu, *abort_flag || !mbar_wait(&bars.hfull[buf], (hb >> 1) & 1, p.err));
+        if (failed) break;
+        tc_fence_after();
+        const uint64_t hdesc = b_tmpl + halo0 + (uint32_t)buf * (p.halo_bytes >> 4);
+        for (int st = 0; st < p.nst; ++st, ++q) {
+          if (seg_left == 0) {
+            // a new accumulation segment: wait until its accumulator is free
+            bi = p.promote ? 0 : (int)(u & 1);
+            const uint32_t use = p.promote ? u : (u >> 1);
+            failed = __any_sync(0xffffffffu, !mbar_wait(&bars.dempty[bi], (use & 1) ^ 1, p.err));
+            if (failed) break;
+            tc_fence_after();
+            seg_left = min(p.seg_stages, tstages - done);
+            first = true;
+          }
+          const int s = q % p.stages;
+          failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[s], (q / p.stages) & 1, p.err));
+          if (failed) break;
+          tc_fence_after();
+          if (elect_one()) {
+            const uint32_t dt = tmem + (uint32_t)bi * kAccCols;
+            const int t0 = st * p.T, t1 = min(g.R * g.S, t0 + p.T);
+            uint64_t sa = a_tmpl + stage0 + (uint32_t)s * stage16;
+            for (int tap = t0; tap < t1; ++tap, sa += chunk16) {
+              const uint64_t hp = hdesc + (uint32_t)p.tap_phase[tap] * TERMS * part16 + (uint32_t)p.tap_off[tap];
+              for (int j = 0; j < p.KS; ++j) {
+#pragma unroll
+                for (int m = 0; m < ML::n; ++m) {
+                  mma_bf16_ss(dt, sa + (uint32_t)ML::arow(m) * row16 + 16u * j,
+                              hp + (uint32_t)ML::bterm(m) * part16 + (uint32_t)j * kstep_b16, idesc,
+                              (first && m == 0) ? 0u : 1u);
+                  first = false;
+                }
+              }
+            }
+            tc_commit(&bars.empty[s]);  // the stage may be refilled once these MMAs are done
+          }
+          __syncwarp();
+          first = false;
+          ++done;
+          if (--seg_left == 0) {
+            if (elect_one()) tc_commit(&bars.dfull[bi]);
+            __syncwarp();
+            ++u;
+          }
+        }
+        if (failed) break;
+        if (elect_one()) tc_commit(&bars.hempty[buf]);  // the halo buffer may be refilled
+        __syncwarp();
+      }
+    }
+    if (failed) *abort_flag = 1;
+    // Every MMA issued retires before tensor and shared memory are released.
+    if (elect_one()) tc_commit(&bars.drain);
+    __syncwarp();
+    mbar_wait(&bars.drain, 0, p.err);
+  } else if (warp == kLoadWarp) {
+    // ------------------------------------------------------------ loader
+    // A bulk copy costs its issuing thread a few hundred cycles whatever its
+    // size, so each stage (T consecutive taps of one plane block, contiguous
+    // in the packed operand) is one copy.
+    if (lane == 0) {
+      const int RS = g.R * g.S;  // taps
+      uint32_t q = 0;
+      bool ok = true;
+      for (int i = blockIdx.x; ok && i < p.total && !*abort_flag; i += gridDim.x) {
+        const Item it = decode(p, i);
+        const uint8_t *src = p.bpack + (size_t)it.nb * p.NCB * RS * p.chunk_bytes;
+        for (int cb = 0; ok && cb < p.NCB; ++cb)
+          for (int st = 0; st < p.nst; ++st, ++q) {
+            const int s = q % p.stages;
+            if (!mbar_wait(&bars.empty[s], ((q / p.stages) & 1) ^ 1, p.err)) {
+              ok = false;
+              break;
+            }
+            const int t0 = st * p.T;
+            const uint32_t bytes = (uint32_t)min(p.T, RS - t0) * p.chunk_bytes;
+            mbar_arrive_expect_tx(&bars.full[s], bytes);
+            bulk_load(stage + (size_t)s * p.stage_bytes, src + ((size_t)cb * RS + t0) * p.chunk_bytes, bytes,
+                      &bars.full[s]);
+          }
+      }
+      if (!ok) *abort_flag = 1;
+      if (*abort_flag) {
+        // copies still in flight land before shared memory is released
+        for (uint32_t qq = q > (uint32_t)p.stages ? q - p.stages : 0; qq < q; ++qq)
+          mbar_wait(&bars.full[qq % p.stages], (qq / p.stages) & 1, p.err);
+      }
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int ew = warp - kEpiWarp0;
+    const int quarter = warp & 3;         // tensor-memory lanes this warp may access
+    const int half = ew >> 2;             // column half
+    const bool big = quarter < 2;         // rows 0-63: hi*hi sums; 64-127: corrections
+    const int pair = (quarter & 1) * 2 + half;  // big warp + small warp of the same filters and columns
+    const int bar_id = 2 + pair;
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    const int ncol = p.N / 2, cbeg = half * ncol;
+    float *xp = xch + pair * 2 * kXchFloats;
+    const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
+    const size_t opl = (size_t)g.OH * g.OW;
+    uint32_t u = 0;
+    bool failed = false;
+    for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
+      const Item it = decode(p, i);
+      const int p0 = it.tile * p.N;
+      const int bw = min(p.BW, g.OW - it.band * p.BW);  // valid columns of the band
+      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)it.band * p.BW;
+      for (int seg = 0; seg < nseg; ++seg, ++u) {
+        const int bi = p.promote ? 0 : (int)(u & 1);
+        const uint32_t use = p.promote ? u : (u >> 1);
+        bool bad = *abort_flag != 0 || !mbar_wait(&bars.dfull[bi], use & 1, p.err);
+        bad = named_sync_or(bar_id, 64, bad);  // both warps of the pair agree
+        if (bad) {
+          failed = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t sc = tmem + lane_base + (uint32_t)bi * kAccCols;
+        const uint32_t rc = tmem + lane_base + kAccCols;  // running sum (promotion)
+        const bool first = seg == 0, last = seg == nseg - 1;
+        if (!last) {
+          // promotion: R (+)= S, FP32 round to nearest
+          for (int c = cbeg; c < cbeg + ncol; c += 16) {
+            uint32_t s16[16], r16[16];
+            tmem_ld16(sc + c, s16);
+            if (!first) tmem_ld16(rc + c, r16);
+            tc_wait_ld();
+            if (!first) {
+#pragma unroll
+              for (int t = 0; t < 16; ++t) s16[t] = __float_as_uint(__uint_as_float(s16[t]) + __uint_as_float(r16[t]));
+            }
+            tmem_st16(rc + c, s16);
+          }
+          tc_wait_st();
+          tc_fence_before();
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&bars.dempty[bi]);
+          continue;
+        }
+        // last segment: out = S (+ R) for the big and the small rows of each
+        // filter, added in shared memory ([filter][16 positions] per chunk);
+        // then the big warp stores two filters' 16 positions per instruction
+        int kb = 0;
+        for (int c = cbeg; c < cbeg + ncol; c += 16, ++kb) {
+          uint32_t s16[16], r16[16];
+          tmem_ld16(sc + c, s16);
+          if (!first) tmem_ld16(rc + c, r16);
+          tc_wait_ld();
+          float v[16];
+#pragma unroll
+          for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(s16[t]) + (first ? 0.0f : __uint_as_float(r16[t]));
+          if (c + 16 >= cbeg + ncol) {  // the accumulator is read: release it
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars.dempty[bi]);
+          }
+          float *xt = xp + (kb & 1) * kXchFloats;  // [32 filters][pitch 17]
+          if (!big) {
+#pragma unroll
+            for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = v[t];
+          }
+          named_sync(bar_id, 64);
+          if (big) {
+            // every load of a batch is issued before the batch's stores
+            float w[16];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) w[t] = xt[lane * kXchPitch + t];
+#pragma unroll
+            for (int t = 0; t < 16; ++t) {
+              w[t] += v[t];
+              if (relu) w[t] = fmaxf(w[t], 0.0f);
+            }
+#pragma unroll
+            for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
+            __syncwarp();
+            if (p.vec4) {
+              // lane -> (filter 8i + lane/4, positions c + 4*(lane%4) .. +3):
+              // four outputs that are consecutive and 16-byte aligned
+              const int t = 4 * (lane & 3);
+              const int G = p0 + c + t;
+              const int Y = G / p.P, X = G - Y * p.P;
+              const bool ok = Y < g.OH && X < bw;
+              const int fbase = it.nb * 64 + (quarter & 1) * 32 + (lane >> 2);
+              float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * g.OW + X;
+#pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                const float *r = xt + (8 * i + (lane >> 2)) * kXchPitch + t;
+                w[4 * i] = r[0];
+                w[4 * i + 1] = r[1];
+                w[4 * i + 2] = r[2];
+                w[4 * i + 3] = r[3];
+              }
+#pragma unroll
+              for (int i = 0; i < 4; ++i)
+                if (ok && fbase + 8 * i < g.groups)
+                  *reinterpret_cast<float4 *>(yo + (size_t)(8 * i) * opl) =
+                      make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+            } else {
+              // lane -> (filter 2i + lane/16, position c + lane%16)
+              const int t = lane & 15;
+              const int G = p0 + c + t;
+              const int Y = G / p.P, X = G - Y * p.P;
+              const bool ok = Y < g.OH && X < bw;
+              const int fbase = it.nb * 64 + (quarter & 1) * 32 + (lane >> 4);
+              float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * g.OW + X;
+#pragma unroll
+              for (int i = 0; i < 16; ++i) w[i] = xt[(2 * i + (lane >> 4)) * kXchPitch + t];
+#pragma unroll
+              for (int i = 0; i < 16; ++i)
+                if (ok && fbase + 2 * i < g.groups) yo[(size_t)(2 * i) * opl] = w[i];
+            }
+          }
+        }
+      }
+    }
+    if (failed) *abort_flag = 1;
+  }
+
+  // ---------------------------------------------------------------- teardown
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kMmaWarp) tmem_dealloc(tmem, 512);
+}
+
+// Pack the filter bank into per-chunk operand images: chunk (nb, cb, tap) =
+// arows x CB bf16, row blocks of 64 as block_term() lists, row n of a block =
+// filter nb*64 + n, column ci = plane cb*CB + ci, the filter value of the
+// tap (flipped for convolution).  Layout: core matrices of 8 rows x 8
+// columns (128 bytes), row groups SBO = CB*16 bytes apart, column groups
+// LBO = 128 bytes apart.  Rows or columns past the real counts are 0.
+__global__ void bank_pack_kernel(ConvGeom g, const float *__restrict__ f, uint8_t *__restrict__ out, int CB,
+                                 int NCB, int nblocks, int terms, int arows) {
+  const int RS = g.R * g.S;
+  const int total = nblocks * NCB * RS * arows * CB;
+  // the previous kernel (the last launch that read the packed operand) must
+  // be done before it is rewritten; the consuming kernel may be scheduled now
+  grid_dependency_wait();
+  allow_dependent_launch();
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    const int ci = idx % CB;
+    int rest = idx / CB;
+    const int row = rest % arows;
+    rest /= arows;
+    const int tap = rest % RS;
+    rest /= RS;
+    const int cb = rest % NCB;
+    const int nb = rest / NCB;
+    const int part = block_term(terms, row >> 6);
+    const int k = nb * 64 + (row & 63), c = cb * CB + ci;
+    float v = 0.0f;
+    if (part >= 0 && k < g.groups && c < g.n) {
+      int ip, fp;
+      plane_pair(g, k, c, &ip, &fp);  // output plane k of image 0, term c
+      const int r = tap / g.S, s = tap - r * g.S;
+      const int src = g.orient == CCT_CONVOLUTION ? (g.R - 1 - r) * g.S + (g.S - 1 - s) : tap;
+      const float a = f[(size_t)fp * RS + src];
+      const float h = __bfloat162float(__float2bfloat16_rn(a));
+      if (part == 0) {
+        v = h;
+      } else if (terms == 2) {
+        v = a - h;  // rounded to bf16 below
+      } else {
+        const float m = __bfloat162float(__float2bfloat16_rn(a - h));
+        v = part == 1 ? m : (a - h) - m;
+      }
+    }
+    const size_t chunk = ((size_t)nb * NCB + cb) * RS + tap;
+    const uint32_t off = (uint32_t)((row >> 3) * (CB * 16) + (ci >> 3) * 128 + (row & 7) * 16 + (ci & 7) * 2);
+    *reinterpret_cast<__nv_bfloat16 *>(out + chunk * ((size_t)arows * CB * 2) + off) = __float2bfloat16_rn(v);
+  }
+}
+
+std::mutex g_bank_mu;
+std::unordered_map<uint64_t, size_t> g_bank_attr;
+
+template <int TERMS>
+int launch_terms(const BankParams &p, cudaStream_t st) {
+  auto kern = bank_tc_kernel<TERMS>;
+  {
+    // Dynamic shared memory above 48 KB needs the opt-in attribute; keep the
+    // largest size set so far per (device, instance).
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)TERMS;
+    std::lock_guard<std::mutex> lk(g_bank_mu);
+    size_t &have = g_bank_attr[key];
+    if (have < p.smem_bytes) {
+      const int rc = check_cuda(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                     (int)p.smem_bytes),
+                                "cudaFuncSetAttribute(bank_tc)");
+      if (rc) return rc;
+      have = p.smem_bytes;
+    }
+  }
+  const int rc = launch_pdl(kern, dim3(p.grid), dim3(kThreads), p.smem_bytes, st, "bank_tc_kernel launch", p);
+  if (rc) return rc;
+  count_launches(1);
+  return check_cuda(cudaGetLastError(), "bank_tc_kernel launch");
+}
+
+int floor_div(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+int pos_mod(int a, int b) { return ((a % b) + b) % b; }
+
+}  // namespace
+
+bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
+  if (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM && g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+    return false;
+  if (terms != 2 && terms != 3) return false;
+  if (g.up != 1 || g.fup != 1 || g.down < 1 || g.down > 2) return false;
+  const int RS = g.R * g.S;
+  if (RS > kBankMaxTaps || g.n < 1 || g.groups < 1) return false;
+  BankParams p{};
+  p.g = g;
+  p.terms = terms;
+  p.nmma = terms == 2 ? 2 : 5;
+  p.arows = terms == 2 ? 192 : 448;
+  const int d = g.down;
+  // row / column shifts in strided units and the input phases the taps read
+  p.sr_min = floor_div(-g.low_r, d);
+  p.sc_min = floor_div(-g.low_c, d);
+  const int dr = floor_div(g.R - 1 - g.low_r, d) - p.sr_min;
+  const int dc = floor_div(g.S - 1 - g.low_c, d) - p.sc_min;
+  int phase_of[2][2] = {{-1, -1}, {-1, -1}};
+  for (int r = 0; r < g.R; ++r)
+    for (int s = 0; s < g.S; ++s) {
+      const int pr = pos_mod(r - g.low_r, d), pc = pos_mod(s - g.low_c, d);
+      if (phase_of[pr][pc] < 0) {
+        phase_of[pr][pc] = p.nphase;
+        p.phase_r[p.nphase] = pr;
+        p.phase_c[p.nphase] = pc;
+        ++p.nphase;
+      }
+    }
+  // Band width BW, tile size N (positions) and plane block CB, by a cost
+  // model: an M=128, 16-deep MMA over N positions takes N/2 tensor cycles and
+  // reads 4 KB of filter plus 32*N bytes of halo from shared memory at about
+  // 128 B per cycle, so its time is max(N/2, 32 + N/4) cycles; each tile also
+  // pays a fixed hand-off (about 8 cycles per k-step).  Grid columns past a
+  // band's outputs are paid for too, and the work items (image, band, tile,
+  // filter block) run in waves of one per SM.  The
+  // plan needs two halo buffers, at least three filter stages and the
+  // epilogue's exchange buffers in shared memory; among equal costs the
+  // larger plane block wins (fewer halo hand-offs).
+  // dynamic shared memory: 227 KB per CTA less the static barriers and exchange buffers
+  const size_t budget = 225 * 1024;
+  const int cmax = ((g.n + 15) / 16) * 16;
+  bool found = false;
+  double best_cost = 0.0;
+  int best_cb = 0;
+  for (int bw : {g.OW, 512, 256, 192, 128, 96, 64, 48, 32}) {
+    if (bw > g.OW || (bw == g.OW && bw > 1024)) continue;
+    const int nbands = (g.OW + bw - 1) / bw;
+    const int BW = (g.OW + nbands - 1) / nbands;  // balanced bands
+    const int P = BW + dc;
+    const long long npos = (long long)g.OH * P;
+    for (int N : {256, 224, 192, 160, 128, 96, 64}) {
+      const long long tiles = (npos + N - 1) / N;
+      const int L = ((N + dr * P + dc) + 7) & ~7;
+      for (int CB : {64, 32, 16}) {
+        if (CB > cmax && CB != 16) continue;
+        const size_t part = (size_t)L * CB * 2;
+        const size_t halo = (((size_t)p.nphase * terms * part) + 127) & ~(size_t)127;
+        const size_t chunk = (size_t)p.arows * CB * 2;
+        // taps per stage: about 1100 cycles of MMAs per bulk copy and per
+        // stage hand-off, at least three stages
+        const double tap_cycles = (CB / 16) * p.nmma * std::max(0.5 * N, 32.0 + 0.25 * N);
+        int T = std::min(RS, std::max(1, (int)std::ceil(1100.0 / tap_cycles)));
+        while (T > 1 && 2 * halo + 3 * T * chunk + kXchBytes > budget) --T;
+        if (2 * halo + 3 * T * chunk + kXchBytes > budget || L * 16 >= (1 << 18)) continue;
+        if (T * tap_cycles < 500.0 && T < RS && CB > 16) continue;  // a smaller plane block keeps stages long
+        // work items run in waves over the SMs: a small problem takes smaller
+        // tiles to occupy more of them
+        const long long items = (long long)g.batch * nbands * tiles * ((g.groups + 63) / 64);
+        const double waves = (double)((items + sms - 1) / sms);
+        const double cost = waves * (std::max(0.5 * N, 32.0 + 0.25 * N) + 8.0);
+        if (!found || cost < best_cost * 0.999 || (cost <= best_cost * 1.001 && CB > best_cb)) {
+          p.nbands = nbands;
+          p.BW = BW;
+          p.P = P;
+          p.N = N;
+          p.CB = CB;
+          p.L = L;
+          p.part_bytes = (uint32_t)part;
+          p.halo_bytes = (uint32_t)halo;
+          p.chunk_bytes = (uint32_t)chunk;
+          p.T = T;
+          p.stage_bytes = (uint32_t)(T * chunk);
+          p.stages = (int)std::min<size_t>(6, (budget - 2 * halo - kXchBytes) / p.stage_bytes);
+          p.tiles_band = (int)tiles;
+          best_cost = cost;
+          best_cb = CB;
+          found = true;
+        }
+        break;  // the largest plane block that fits
+      }
+    }
+  }
+  if (!found) return false;
+  for (int tap = 0; tap < RS; ++tap) {
+    const int r = tap / g.S, s = tap % g.S;
+    const int ar = r - g.low_r, ac = s - g.low_c;
+    p.tap_phase[tap] = phase_of[pos_mod(ar, d)][pos_mod(ac, d)];
+    p.tap_off[tap] = (floor_div(ar, d) - p.sr_min) * p.P + (floor_div(ac, d) - p.sc_min);
+  }
+  p.nblocks = (g.groups + 63) / 64;
+  p.NCB = (g.n + p.CB - 1) / p.CB;
+  p.KS = p.CB / 16;
+  p.nst = (RS + p.T - 1) / p.T;
+  const int tstages = p.NCB * p.nst;
+  // Promotion: the hi*hi accumulator takes at most 64 k-steps (1024 terms of
+  // the reduction) before it is added into the FP32 running sum.
+  const int kmax = 64;
+  p.promote = p.NCB * RS * p.KS > kmax ? 1 : 0;
+  p.seg_stages = p.promote ? std::max(1, kmax / (p.T * p.KS)) : tstages;
+  // float4 stores: groups of 4 grid positions (p0 and N are multiples of 4)
+  // never straddle a grid row or the band's last output column, and land on
+  // 16-byte aligned outputs
+  p.vec4 = (p.P % 4 == 0 && p.BW % 4 == 0 && g.OW % 4 == 0 && p.N % 4 == 0) ? 1 : 0;
+  p.total = g.batch * p.nbands * p.tiles_band * p.nblocks;
+  if (p.total < 1) return false;
+  p.grid = std::min(p.total, sms);
+  p.smem_bytes = 2 * (size_t)p.halo_bytes + (size_t)p.stages * p.stage_bytes;
+  p.pack_bytes = (size_t)p.nblocks * p.NCB * RS * p.chunk_bytes;
+  *out = p;
+  return true;
+}
+
+int launch_bank_pack(const BankParams &p, const float *f, uint8_t *packed, cudaStream_t st) {
+  const long long total = (long long)p.nblocks * p.NCB * p.g.R * p.g.S * p.arows * p.CB;
+  if (total > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "packed filter operand too large");
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+  const int rc = launch_pdl(bank_pack_kernel, dim3(blocks), dim3(256), 0, st, "bank_pack_kernel launch", p.g, f,
+                            packed, p.CB, p.NCB, p.nblocks, p.terms, p.arows);
+  if (rc) return rc;
+  count_launches(1);
+  return check_cuda(cudaGetLastError(), "bank_pack_kernel launch");
+}
+
+int launch_bank_tc(const BankParams &p, const float *x, float *y, const uint8_t *packed, unsigned *err,
+                   cudaStream_t st) {
+  BankParams q = p;
+  q.x = x;
+  q.y = y;
+  if ((reinterpret_cast<uintptr_t>(y) & 15) != 0) q.vec4 = 0;  // float4 stores need a 16-byte aligned output
+  q.bpack = packed;
+  q.err = err;
+  return p.terms == 2 ? launch_terms<2>(q, st) : launch_terms<3>(q, st);
+}
+
+}  // namespace cct
+
+namespace cct {
+
+bool frame_tc_choose(const ConvGeom &g, int precision, int sms, FrameTcChoice *out) {
+  FrameTcChoice c{};
+  if (precision == CCT_PREC_BF16X3 && g.groups <= 32 && frame_tc_plan(g, sms, &c.tp)) {
+    c.bank = false;
+    c.pack_bytes = c.tp.pack_bytes;
+  } else if (bank_tc_plan(g, precision == CCT_PREC_BF16X6 ? 3 : 2, sms, &c.bp)) {
+    c.bank = true;
+    c.pack_bytes = c.bp.pack_bytes;
+  } else if (precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &c.tp)) {
+    c.bank = false;
+    c.pack_bytes = c.tp.pack_bytes;
+  } else {
+    return false;
+  }
+  *out = c;
+  return true;
+}
+
+int frame_tc_pack(const FrameTcChoice &c, const float *f, uint8_t *packed, cudaStream_t st) {
+  return c.bank ? launch_bank_pack(c.bp, f, packed, st) : launch_pack_filters(c.tp, f, packed, st);
+}
+
+int frame_tc_run(const FrameTcChoice &c, const float *x, float *y, const uint8_t *packed, unsigned *err,
+                 cudaStream_t st) {
+  if (c.bank) return launch_bank_tc(c.bp, x, y, packed, err, st);
+  if ((reinterpret_cast<uintptr_t>(x) & 15) != 0)
+    return set_error(CCT_EINVAL, "image pointer must be 16-byte aligned for the tensor-core path");
+  return launch_frame_tc(c.tp, x, y, packed, err, st);
+}
+
+}  // namespace cct

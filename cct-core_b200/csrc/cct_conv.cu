@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "cct_internal.h"
+#include "bank_tc.h"
 #include "fft_conv.h"
 #include "frame_tc.h"
 
@@ -82,7 +83,7 @@ static int resolve(const cct_conv_desc *d, ConvGeom *g) {
     return set_error(CCT_EINVAL, "bad filter orientation %d", d->orientation);
   if (d->vector_mode < CCT_PLANE_BY_PLANE || d->vector_mode > CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM)
     return set_error(CCT_EINVAL, "bad vector mode %d", d->vector_mode);
-  if (d->precision != CCT_PREC_FP32 && d->precision != CCT_PREC_BF16X3)
+  if (d->precision != CCT_PREC_FP32 && d->precision != CCT_PREC_BF16X3 && d->precision != CCT_PREC_BF16X6)
     return set_error(CCT_EINVAL, "bad precision %d", d->precision);
   if (d->algo < CCT_ALGO_AUTO || d->algo > CCT_ALGO_FFT)
     return set_error(CCT_EINVAL, "bad algorithm %d", d->algo);
@@ -212,7 +213,7 @@ struct cct_conv_plan {
   unsigned *err;  // device error word of `device`
   size_t x_elems, f_elems, y_elems;
   float *static_filter;  // device copy of a static filter, or null
-  TcParams tc;           // tensor-core tile plan (ALGO_FRAME_BF16X3)
+  FrameTcChoice tc;      // tensor-core frame kernel and tile plan (ALGO_FRAME_BF16X3)
   uint8_t *packed;       // packed bf16 hi/lo filter operand (plan workspace)
   bool packed_static;    // packed holds the static filter
   FftParams fft;         // FFT plan (ALGO_FFT)
@@ -316,19 +317,21 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
       use_fft = fft_s < direct_s;
     }
   }
-  TcParams tc{};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool fa_reduce = g.mode == CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM;
   if (d->precision == CCT_PREC_BF16X3 && !reduce && !fa_reduce)
     return set_error(CCT_EINVAL, "BF16X3 precision applies to the BlockReduceSum modes only");
+  if (d->precision == CCT_PREC_BF16X6 && !reduce)
+    return set_error(CCT_EINVAL, "BF16X6 precision applies to the frame BlockReduceSum modes only");
+  FrameTcChoice tc{};
   if (use_fft)
     algo = ALGO_FFT;
   else if (d->precision == CCT_PREC_BF16X3 && fa_reduce && fa_tc_supported(g))
     algo = ALGO_FILTER_ADJOINT_BF16X3;
   else if (fa_f32_supported(g))
     algo = ALGO_FILTER_ADJOINT;
-  else if (d->precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &tc))
+  else if (d->precision != CCT_PREC_FP32 && frame_tc_choose(g, d->precision, sms, &tc))
     algo = ALGO_FRAME_BF16X3;
   else
     algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
@@ -434,7 +437,7 @@ int cct_conv_plan_set_static_filter(cct_conv_plan *p, const float *host_filter) 
     p->fft_static = true;
   }
   if (p->algo == ALGO_FRAME_BF16X3) {
-    rc = launch_pack_filters(p->tc, p->static_filter, p->packed, 0);
+    rc = frame_tc_pack(p->tc, p->static_filter, p->packed, 0);
     if (!rc) rc = check_cuda(cudaStreamSynchronize(0), "pack static filter");
     if (rc) return rc;
     p->packed_static = true;
@@ -449,12 +452,10 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
   cudaStream_t st = (cudaStream_t)stream;
   switch (p->algo) {
     case ALGO_FRAME_BF16X3: {
-      if ((reinterpret_cast<uintptr_t>(x) & 15) != 0)
-        return set_error(CCT_EINVAL, "image pointer must be 16-byte aligned for the tensor-core path");
       int rc = CCT_OK;
-      if (f != p->static_filter || !p->packed_static) rc = launch_pack_filters(p->tc, f, p->packed, st);
+      if (f != p->static_filter || !p->packed_static) rc = frame_tc_pack(p->tc, f, p->packed, st);
       if (rc) return rc;
-      return launch_frame_tc(p->tc, x, y, p->packed, p->err, st);
+      return frame_tc_run(p->tc, x, y, p->packed, p->err, st);
     }
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);

@@ -34,8 +34,8 @@
 //    cudaDeviceReset.
 #include <mutex>
 
+#include "bank_tc.h"
 #include "cct_internal.h"
-#include "frame_tc.h"
 
 namespace {
 
@@ -75,8 +75,6 @@ extern "C" int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *imag
       (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM && g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM))
     return set_error(CCT_ENOTSUP,
                      "the allocation-free entry point runs the BF16X3 BlockReduceSum frame kernel only");
-  if ((reinterpret_cast<uintptr_t>(image) & 15) != 0)
-    return set_error(CCT_EINVAL, "image pointer must be 16-byte aligned");
 
   int dev = 0, major = 0, sms = 0;
   rc = check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
@@ -86,10 +84,9 @@ extern "C" int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *imag
   if (major != 10) return set_error(CCT_ENODEV, "device %d is not sm_100 (major %d)", dev, major);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
-  TcParams tc;
-  if (!frame_tc_plan(g, sms, &tc))
-    return set_error(CCT_ENOTSUP, "shape outside the tensor-core frame kernel (border, sampling, "
-                                  "width or tile size)");
+  FrameTcChoice tc;  // the same kernel and tile plan a plan for this descriptor runs
+  if (!frame_tc_choose(g, CCT_PREC_BF16X3, sms, &tc))
+    return set_error(CCT_ENOTSUP, "shape outside the tensor-core frame kernels (sampling or tile size)");
   if (tc.pack_bytes > kNoAllocScratchBytes)
     return set_error(CCT_EINVAL,
                      "packed filter operand needs %zu bytes; the allocation-free entry point holds "
@@ -102,7 +99,7 @@ extern "C" int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *imag
   unsigned *status = device_error_word();
   if (!status) return set_error(CCT_ECUDA, "device error word: symbol address lookup failed");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  rc = launch_pack_filters(tc, filter, scratch, st);
+  rc = frame_tc_pack(tc, filter, scratch, st);
   if (rc) return rc;
-  return launch_frame_tc(tc, image, out, scratch, status, st);
+  return frame_tc_run(tc, image, out, scratch, status, st);
 }

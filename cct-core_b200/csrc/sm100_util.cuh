@@ -106,6 +106,11 @@ __device__ __forceinline__ bool named_sync_or(int id, int count, bool pred) {
   return r != 0;
 }
 
+// Named barrier over `count` threads (ids 1..15).
+__device__ __forceinline__ void named_sync(int id, int count) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(count) : "memory");
+}
+
 // 3-D tiled TMA load (x innermost) into shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
                                             int x, int y, int z) {
@@ -290,6 +295,18 @@ __device__ __forceinline__ void split_bf16x2(float a, float b, uint32_t &hi, uin
   const float ha = __uint_as_float(hi << 16);
   const float hb = __uint_as_float(hi & 0xFFFF0000u);
   asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(lo) : "f"(b - hb), "f"(a - ha));
+}
+
+// Three-term split: a = ah + am + al with each term bf16 (round to nearest),
+// am the rounded residual of ah and al the rounded residual of ah + am.  The
+// residuals a - ah and a - ah - am are exact in FP32 (Sterbenz), so the three
+// terms carry 24 significant bits of a.
+__device__ __forceinline__ void split3_bf16x2(float a, float b, uint32_t &hi, uint32_t &mid, uint32_t &lo) {
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(hi) : "f"(b), "f"(a));
+  const float ra = a - __uint_as_float(hi << 16), rb = b - __uint_as_float(hi & 0xFFFF0000u);
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(mid) : "f"(rb), "f"(ra));
+  const float sa = ra - __uint_as_float(mid << 16), sb = rb - __uint_as_float(mid & 0xFFFF0000u);
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;\n" : "=r"(lo) : "f"(sb), "f"(sa));
 }
 
 }  // namespace cct

@@ -68,8 +68,13 @@ enum { CCT_PLANE_BY_PLANE = 0, CCT_PROJECT_FRAME = 1,
  * hi*hi + hi*lo + lo*hi products on tcgen05 tensor cores in FP32.  BF16X3
  * applies to the BlockReduceSum modes: the frame modes (PROJECT_FRAME_ and
  * BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM) and FILTER_ADJOINT_BLOCK_REDUCE_SUM
- * (the weight gradient, with BorderValid and no sampling). */
-enum { CCT_PREC_FP32 = 0, CCT_PREC_BF16X3 = 1 };
+ * (the weight gradient, with BorderValid and no sampling).  BF16X6 (frame
+ * modes only) splits each operand into three bf16 terms hi+mid+lo and sums
+ * the six products down to 2^-16 of hi*hi (hh, hm, mh, hl, lh, mm): FP32-level
+ * accuracy for compositions such as a stack of layers, at about twice the
+ * tensor work of BF16X3.  Shapes the tensor-core kernels do not take run on
+ * the FP32 kernels. */
+enum { CCT_PREC_FP32 = 0, CCT_PREC_BF16X3 = 1, CCT_PREC_BF16X6 = 2 };
 /* Direct vs FFT (ConvolutionFFTUsePolicy.scala:24-28 UseFFTNever/Always/WhenBest) */
 enum { CCT_ALGO_AUTO = 0, CCT_ALGO_DIRECT = 1, CCT_ALGO_FFT = 2 };
 /* flags */

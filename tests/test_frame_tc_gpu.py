@@ -21,8 +21,8 @@ def _desc(od, precision=_lib.PREC_BF16X3, flags=0):
                          precision=precision, flags=flags)
 
 
-def run_tc(od, x, f, flags=0, expect_tc=True):
-    plan = _lib.Plan(_desc(od, flags=flags))
+def run_tc(od, x, f, flags=0, expect_tc=True, precision=_lib.PREC_BF16X3):
+    plan = _lib.Plan(_desc(od, precision=precision, flags=flags))
     if expect_tc:
         assert plan.algo == _lib.PLAN_FRAME_BF16X3
     orows, ocols, oplanes = plan.shape
@@ -36,13 +36,13 @@ def run_tc(od, x, f, flags=0, expect_tc=True):
     return yd.cpu().numpy()
 
 
-def check(y, od, x, f, relu=False):
+def check(y, od, x, f, relu=False, tol=TOL):
     ref = O.conv(od, x, f, np.float64)
     if relu:
         ref = np.maximum(ref, 0)
     assert not np.isnan(y).any()
     mx, rms = O.rel_errors(y, ref)
-    assert mx <= TOL, (mx, rms)
+    assert mx <= tol, (mx, rms)
     return mx, rms
 
 
@@ -84,6 +84,22 @@ TC_CASES = [
     (44, 48, 24, 72, 2, 5, O.ZERO, O.DOWN, 2, O.BACKPROJECT_REDUCE),
     # a 208-wide halo: 16-plane blocks (two 32-plane halo buffers do not fit)
     (24, 200, 32, 64, 1, 5, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    # border policies the halo loads map per element (ConvolveHyperKernel.scala:235-317)
+    (30, 31, 20, 70, 2, 7, O.CLAMP, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (30, 30, 20, 70, 2, 7, O.CLAMP, O.DOWN, 2, O.PROJECT_REDUCE),
+    (30, 30, 20, 70, 2, 3, O.CYCLIC, O.DOWN, 2, O.PROJECT_REDUCE),
+    (40, 44, 17, 130, 2, 5, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (33, 37, 5, 7, 3, 3, O.VALID, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (33, 37, 5, 7, 3, 3, O.FULL, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
+    (21, 23, 12, 20, 2, 5, O.CLAMP, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
+    # odd widths (no 16-byte rule on the halo loads) and 1-wide fields
+    (9, 9, 1, 1, 1, 9, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (1, 300, 8, 8, 1, 1, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (300, 1, 8, 8, 1, 1, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    # fields wider than one band of output columns
+    (64, 520, 16, 16, 1, 5, O.CLAMP, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (40, 1027, 4, 16, 1, 9, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (64, 64, 32, 64, 2, 11, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
 ]
 
 
@@ -118,12 +134,47 @@ def test_tc_relu_and_static_filter():
 
 
 def test_tc_unsupported_shapes_use_fp32_kernel():
-    # Clamp border is outside the tensor-core path: the plan picks the exact FP32 kernel.
-    od = O.make_desc(16, 16, 3, 3, planes=8, f_planes=16, batch=1, border=O.CLAMP,
-                     orient=O.XCORR, mode=O.PROJECT_REDUCE)
+    # DownsampleOutput(3) is outside the tensor-core kernels: the plan takes an
+    # FP32 kernel, bit-exact with the FP32 oracle.
+    rng = np.random.default_rng(3)
+    od = O.make_desc(18, 18, 3, 3, planes=8, f_planes=16, batch=1, border=O.CLAMP,
+                     orient=O.XCORR, sampling=O.DOWN, step=3, mode=O.PROJECT_REDUCE)
+    x = rng.standard_normal((8, 18, 18)).astype(np.float32)
+    f = rng.standard_normal((16, 3, 3)).astype(np.float32)
+    y = run_tc(od, x, f, expect_tc=False)
     plan = _lib.Plan(_desc(od))
-    assert plan.algo == _lib.PLAN_FRAME_F32
+    assert plan.algo in (_lib.PLAN_FRAME_F32, _lib.PLAN_DIRECT)
     plan.close()
+    assert np.array_equal(y, O.conv(od, x, f))
+
+
+# Three-term split (BF16X6): the six products down to 2^-16 of hi*hi, with the
+# hi*hi accumulator promoted into an FP32 running sum every 64 k-steps, so the
+# error stays near FP32 level whatever the reduction length.
+X6_TOL = 3e-6
+X6_CASES = [
+    # (H, W, C, K, B, R, border, sampling, step, mode)
+    (28, 28, 512, 512, 1, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),   # a 4608-long reduction
+    (56, 56, 256, 256, 1, 3, O.ZERO, O.DOWN, 2, O.PROJECT_REDUCE),
+    (64, 64, 32, 64, 2, 5, O.ZERO, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
+    (40, 44, 17, 70, 2, 5, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (48, 48, 3, 64, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+]
+
+
+@pytest.mark.parametrize("H,W,C,K,B,R,border,samp,step,mode", X6_CASES)
+def test_tc_three_term_split(H, W, C, K, B, R, border, samp, step, mode):
+    rng = np.random.default_rng(H + 3 * C + K)
+    if mode == O.PROJECT_REDUCE:
+        planes, orient = B * C, O.XCORR
+    else:
+        planes, orient = B * K, O.CONV
+    od = O.make_desc(H, W, R, R, planes=planes, f_planes=K * C, batch=B, border=border,
+                     orient=orient, sampling=samp, step=step, mode=mode)
+    x = rng.standard_normal((planes, H, W)).astype(np.float32)
+    f = (rng.standard_normal((K * C, R, R)) * np.sqrt(2.0 / (C * R * R))).astype(np.float32)
+    mx, rms = check(run_tc(od, x, f, precision=_lib.PREC_BF16X6), od, x, f, tol=X6_TOL)
+    print(f"BF16X6 {H}x{W} C{C} K{K}: normwise max {mx:.3e} rms {rms:.3e}")
 
 
 def test_tc_repeatable():

@@ -191,3 +191,35 @@ def test_eight_layer_stack_224_batch1():
         assert O.rel_errors(got.reshape(ref.shape), ref)[0] <= TOL, i + 1
         prev = got
     stack.close()
+
+
+def test_eight_layer_stack_batch8_three_term_split_end_to_end():
+    """The 224x224x3 eight-layer stack at batch 8 in the three-term split
+    (BF16X6): the last layer's output, after all eight layers from the input,
+    within 1e-5 (normwise) of the same stack in FP64 (zero-border 3x3
+    cross-correlations, DownsampleOutput(2) on layers 2, 4 and 6, ReLU
+    between layers).  The two-term split (BF16X3) keeps each layer under
+    1e-5 but compounds to about 1.4e-5 over eight layers."""
+    import torch.nn.functional as F
+    B = 8
+    stack = eight_layer_stack(B, _lib.PREC_BF16X6)
+    filters = _filters(stack, 21)
+    stack.set_filters(filters)
+    x = np.random.default_rng(22).uniform(-1, 1, stack.field_shapes[0]).astype(np.float32)
+    stack.input.copy_(torch.from_numpy(x))
+    stack.step()
+    torch.cuda.synchronize()
+    assert _lib.LIB.cct_device_status() == _lib.OK
+    got = stack.output.double().reshape(B, 512, 28, 28)
+    a = torch.from_numpy(x).cuda().double().reshape(B, 3, 224, 224)
+    for i, d in enumerate(stack.descs):
+        k = d.filter_planes // (d.image_planes // B)
+        w = torch.from_numpy(filters[i]).cuda().double().reshape(k, d.image_planes // B, 3, 3)
+        a = F.conv2d(a, w, padding=1, stride=d.step if d.sampling == _lib.SAMPLE_DOWN else 1)
+        if d.flags & _lib.FLAG_RELU:
+            a = a.clamp_min(0)
+    err = ((got - a).abs().max() / a.abs().max()).item()
+    rms = ((got - a).pow(2).mean() / a.pow(2).mean()).sqrt().item()
+    print(f"eight-layer stack, batch 8, BF16X6: normwise max {err:.3e} rms {rms:.3e}")
+    assert err <= TOL, err
+    stack.close()

@@ -73,6 +73,7 @@ def test_noalloc_matches_plan_entry_point(H, W, R, planes, fplanes, batch, orien
         assert not torch.isnan(y).any()
         err = (y.double() - r).abs().max().item() / r.abs().max().item()
         assert err <= TOL, err
+        assert torch.equal(y, ref)  # the same kernel and tile plan as the plan entry point
 
 
 def test_noalloc_rejects_filter_banks_beyond_the_limit():
@@ -87,11 +88,12 @@ def test_noalloc_rejects_filter_banks_beyond_the_limit():
 
 
 def test_noalloc_only_takes_the_tensor_core_frame_kernel():
-    desc = _desc(16, 16, 3, 4, 8, 1, _lib.CROSS_CORRELATION, _lib.PROJECT_FRAME_BLOCK_REDUCE_SUM,
-                 border=_lib.BORDER_CLAMP)
-    x = torch.zeros((4, 16, 16), device="cuda")
+    # DownsampleOutput(3) is outside the tensor-core frame kernels
+    desc = _desc(18, 18, 3, 4, 8, 1, _lib.CROSS_CORRELATION, _lib.PROJECT_FRAME_BLOCK_REDUCE_SUM,
+                 down=3)
+    x = torch.zeros((4, 18, 18), device="cuda")
     f = torch.zeros((8, 3, 3), device="cuda")
-    y = torch.zeros((2, 16, 16), device="cuda")
+    y = torch.zeros((2, 6, 6), device="cuda")
     assert _run_noalloc(desc, x, f, y) == _lib.ENOTSUP
 
 

@@ -416,6 +416,27 @@ def plain_workload():
         return {"ms": round(t_sm * 1e3, 4), "GFLOP/s": round(2 * 1024 * 1024 * 64 * 49 / t_sm / 1e9, 1),
                 "color": {"ms": round(t_c * 1e3, 4),
                           "pixels/s": round(2048 * 2048 / t_c, 1)}}
+    def unfused_frame():
+        """projectFrame without the block reduce (CogFunctionAPI.scala:1370-1377):
+        B=4 images of C=32 planes, 64 filters of 5x5x32, every (image, filter
+        plane) pair an output plane: 8192 planes of 64x64 from 128 input
+        planes, on the FP32 frame kernel without its reduce; HBM-bound on the output."""
+        Bu, Cu, Ku, Hu, Wu, Ru = 4, 32, 64, 64, 64, 5
+        pl = _lib.Plan(C.make_desc((Hu, Wu, Bu * Cu), (Ru, Ru, Ku * Cu), C.BorderZero, _lib.CROSS_CORRELATION,
+                                   C.NoSamplingConvolution, _lib.PROJECT_FRAME, Bu))
+        xu = torch.empty((Bu * Cu, Hu, Wu), device="cuda").uniform_(-1, 1, generator=gen)
+        fu = torch.empty((Ku * Cu, Ru, Ru), device="cuda").uniform_(-1, 1, generator=gen)
+        yu = torch.empty((Bu * Ku * Cu, Hu, Wu), device="cuda")
+        t = time_single_launch(lambda: pl.run(xu.data_ptr(), fu.data_ptr(), yu.data_ptr(), stream), reps=10)
+        byts = 4 * (xu.numel() + fu.numel() + yu.numel())
+        torch.cuda.synchronize()
+        ref = np_conv_same(xu[:1].double().cpu().numpy(), fu[:1].double().cpu().numpy()[:, None], flip=False)
+        err = errors_vs(yu[:1].cpu().numpy(), ref)
+        algo = pl.algo
+        pl.close()
+        return {"ms": round(t * 1e3, 4), "GB/s": round(byts / t / 1e9, 1),
+                "hbm_frac": round(byts / t / 1e9 / load_peaks()[0]["hbm_gbs"], 4), "plan_algo": algo,
+                "error_vs_fp64": dict(err, sample="output plane 0")}
     sep_bytes = 2 * 4 * P * H * W
     step()
     torch.cuda.synchronize()
@@ -424,7 +445,8 @@ def plain_workload():
              "single_plane_256x256_us": round(single_s * 1e6, 2),
              "separable_5+5_4096x256x256": {"ms": round(sep_s * 1e3, 4),
                                             "GB/s": round(sep_bytes / sep_s / 1e9, 1)},
-             "scalar_matrix_1024x1024_8x8_of_7x7": other_ops()}
+             "scalar_matrix_1024x1024_8x8_of_7x7": other_ops(),
+             "project_frame_unfused_4x32x64_64x64_5x5": unfused_frame()}
     extra["color_2048x2048_5x5"] = extra["scalar_matrix_1024x1024_8x8_of_7x7"].pop("color")
 
     byts = 4 * (2 * P * H * W + R * R)
@@ -705,7 +727,7 @@ class ServeBench:
     def run(self, per_call, rate, n):
         import numpy as np
         from cctconv.serve import Server
-        server = Server(slots=4, max_batch=64, arena_bytes=16 << 30, per_call=per_call)
+        server = Server(slots=4, max_batch=64, per_call=per_call)  # admission by free HBM
         reqs, flops, hbytes = self.build(server)
         reqs, k = reqs[:n], n / len(reqs)
         arrivals = np.cumsum(np.random.default_rng(int(rate)).exponential(1.0 / rate, n))

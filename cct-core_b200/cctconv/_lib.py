@@ -58,7 +58,7 @@ class CctError(RuntimeError):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("struct_size", ctypes.c_int32), ("slots", ctypes.c_int32),
                 ("max_batch", ctypes.c_int32), ("flags", ctypes.c_int32),
-                ("arena_bytes", ctypes.c_uint64)]
+                ("arena_bytes", ctypes.c_uint64), ("hbm_reserve_bytes", ctypes.c_uint64)]
 
 
 class ServeRequest(ctypes.Structure):

@@ -1,8 +1,8 @@
 """Request serving over libcctconv (cct_server_*).
 
-A ``Server`` owns an HBM arena and a scheduler thread in the library:
+A ``Server`` owns a scheduler thread and device memory claimed from free HBM:
 requests (a convolution with host buffers, or one step of a resident
-``LayerStack`` graph) are admitted as arena room frees up and batched into
+``LayerStack`` graph) are admitted as device memory frees up and batched into
 persistent launches, with several launches in flight.  ``per_call=True``
 gives the plain per-call dispatch serving is compared with: one request at a
 time, synchronised.
@@ -35,10 +35,15 @@ def graph_request(graph, image_ptr, out_ptr):
 
 
 class Server:
-    def __init__(self, slots=3, max_batch=64, arena_bytes=8 << 30, per_call=False):
+    def __init__(self, slots=3, max_batch=64, arena_bytes=0, per_call=False, hbm_reserve_bytes=0):
+        """arena_bytes: cap on the device memory the server holds (0: none,
+        requests are admitted by the device's free HBM less
+        hbm_reserve_bytes, 0 meaning the library's 2 GiB)."""
         cfg = _lib.ServerConfig()
         _lib.LIB.cct_server_config_init(ctypes.byref(cfg))
         cfg.slots, cfg.max_batch, cfg.arena_bytes = slots, max_batch, arena_bytes
+        if hbm_reserve_bytes:
+            cfg.hbm_reserve_bytes = hbm_reserve_bytes
         cfg.flags = _lib.SERVE_PER_CALL if per_call else 0
         h = ctypes.c_void_p()
         _lib.check(_lib.LIB.cct_server_create(ctypes.byref(cfg), ctypes.byref(h)))

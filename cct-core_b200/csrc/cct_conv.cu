@@ -5,6 +5,7 @@
 // DynamicConvolutionGenerator.convolveDirectly
 // (generator/DynamicConvolutionGenerator.scala:484-539).
 #include <atomic>
+#include <map>
 #include <mutex>
 #include <cstdarg>
 #include <cstdio>
@@ -289,6 +290,95 @@ static int current_sm100(int *dev) {
   return CCT_OK;
 }
 
+// Direct vs FFT for UseFFTWhenBest.  The reference decides from a timing
+// table measured offline per field and filter size
+// (generator/FFTConvolutionUtils.scala:100-142, 145-236); here the two
+// kernels are timed on the device itself, once per (device, field size,
+// filter size, border), on one plane, and the decision is cached for the
+// process.  Both paths cost the same per plane, so one plane decides for
+// any plane count.  The FFT is timed with a static filter (its spectrum made
+// once, as for the reference's constant filters).  The direct kernels keep
+// the reference's FP32 arithmetic bit for bit, so the FFT is taken only when
+// it is clearly faster: at least 1.2x when measured, never for launch-bound
+// planes (direct under 5 us by the model), and without measuring where the
+// modelled times differ tenfold.
+static int time_plan_us(cct_conv_plan *p, const float *x, const float *f, float *y, cudaStream_t st, float *us);
+static bool fft_measured_faster(const cct_conv_desc *d, const ConvGeom &g, const FftParams &fp, int dev) {
+  const double direct_s = 2.0 * g.OH * g.OW * g.R * g.S / 30e12 + 3e-6;
+  const double fft_s = 24.0 * fp.Fr * fp.Fc / 2e12 + 12e-6;
+  if (direct_s < 5e-6) return false;
+  if (direct_s > 10.0 * fft_s) return true;
+  if (fft_s > 10.0 * direct_s) return false;
+  static std::mutex mu;
+  static std::map<std::vector<int>, bool> cache;
+  const std::vector<int> key = {dev, g.H, g.W, g.R, g.S, g.border};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  bool fft_faster = fft_s < direct_s;  // the model, should a measurement fail
+  cct_conv_desc one = *d;
+  one.image_planes = 0;
+  one.filter_planes = 0;
+  one.batch_size = 1;
+  one.vector_mode = CCT_PLANE_BY_PLANE;
+  one.precision = CCT_PREC_FP32;
+  one.flags = 0;
+  cct_conv_plan *pd = nullptr, *pf = nullptr;
+  float *x = nullptr, *f = nullptr, *y = nullptr;
+  cudaStream_t st = nullptr;
+  float td = 0.0f, tf = 0.0f;
+  one.algo = CCT_ALGO_DIRECT;
+  int rc = cct_conv_plan_create(&one, &pd);
+  one.algo = CCT_ALGO_FFT;
+  if (!rc) rc = cct_conv_plan_create(&one, &pf);
+  if (!rc) rc = check_cuda(cudaMalloc(&x, sizeof(float) * (size_t)g.H * g.W), "triage buffers");
+  if (!rc) rc = check_cuda(cudaMalloc(&y, sizeof(float) * (size_t)g.OH * g.OW), "triage buffers");
+  if (!rc) rc = check_cuda(cudaMalloc(&f, sizeof(float) * (size_t)g.R * g.S), "triage buffers");
+  if (!rc) rc = check_cuda(cudaMemset(x, 0, sizeof(float) * (size_t)g.H * g.W), "triage buffers");
+  if (!rc) rc = check_cuda(cudaMemset(f, 0, sizeof(float) * (size_t)g.R * g.S), "triage buffers");
+  if (!rc) {
+    std::vector<float> hf((size_t)g.R * g.S, 0.0f);
+    rc = cct_conv_plan_set_static_filter(pf, hf.data());
+  }
+  if (!rc) rc = check_cuda(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "triage stream");
+  if (!rc) rc = time_plan_us(pd, x, f, y, st, &td);
+  if (!rc) rc = time_plan_us(pf, x, nullptr, y, st, &tf);
+  if (!rc) fft_faster = 1.2f * tf < td;
+  if (st) cudaStreamDestroy(st);
+  cudaFree(x);
+  cudaFree(y);
+  cudaFree(f);
+  cct_conv_plan_destroy(pd);
+  cct_conv_plan_destroy(pf);
+  if (!rc) {
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = fft_faster;
+  }
+  return fft_faster;
+}
+
+static int time_plan_us(cct_conv_plan *p, const float *x, const float *f, float *y, cudaStream_t st, float *us) {
+  for (int i = 0; i < 2; ++i) {
+    const int rc = cct_conv_run(p, x, f, y, st);
+    if (rc) return rc;
+  }
+  cudaEvent_t a = nullptr, b = nullptr;
+  int rc = check_cuda(cudaEventCreate(&a), "triage event");
+  if (!rc) rc = check_cuda(cudaEventCreate(&b), "triage event");
+  if (!rc) rc = check_cuda(cudaEventRecord(a, st), "triage event");
+  for (int i = 0; i < 5 && !rc; ++i) rc = cct_conv_run(p, x, f, y, st);
+  if (!rc) rc = check_cuda(cudaEventRecord(b, st), "triage event");
+  if (!rc) rc = check_cuda(cudaEventSynchronize(b), "triage event");
+  float ms = 0.0f;
+  if (!rc) rc = check_cuda(cudaEventElapsedTime(&ms, a, b), "triage event");
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  *us = ms * 200.0f;  // per run, microseconds
+  return rc;
+}
+
 int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   if (!out) return set_error(CCT_EINVAL, "null plan output");
   *out = nullptr;
@@ -305,18 +395,11 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   // Direct vs FFT (DynamicConvolutionGenerator.scala:109-150): the FFT takes
   // plane-by-plane convolutions without sampling under Zero/Clamp/Cyclic;
   // UseFFTAlways falls back to the direct kernels outside that, as the
-  // reference does; WhenBest compares modelled times.
+  // reference does; WhenBest takes the path measured faster on this device.
   FftParams fp{};
   bool use_fft = false;
-  if (d->algo != CCT_ALGO_DIRECT && fft_plan(g, &fp)) {
-    if (d->algo == CCT_ALGO_FFT) {
-      use_fft = true;
-    } else {
-      const double direct_s = 2.0 * g.OH * g.OW * g.R * g.S * (double)g.pout / 30e12 + 3e-6;
-      const double fft_s = 24.0 * fp.Fr * fp.Fc * (double)g.pout / 2e12 + 12e-6;
-      use_fft = fft_s < direct_s;
-    }
-  }
+  if (d->algo != CCT_ALGO_DIRECT && fft_plan(g, &fp))
+    use_fft = d->algo == CCT_ALGO_FFT || fft_measured_faster(d, g, fp, dev);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool fa_reduce = g.mode == CCT_FILTER_ADJOINT_BLOCK_REDUCE_SUM;
@@ -334,7 +417,9 @@ int cct_conv_plan_create(const cct_conv_desc *d, cct_conv_plan **out) {
   else if (d->precision != CCT_PREC_FP32 && frame_tc_choose(g, d->precision, sms, &tc))
     algo = ALGO_FRAME_BF16X3;
   else
-    algo = (reduce && frame_f32_supported(g)) ? ALGO_FRAME_F32 : ALGO_DIRECT;
+    // the FP32 frame kernel: fused and unfused frame modes (with the reduce
+    // or each input plane's result to its own output plane)
+    algo = frame_f32_supported(g) ? ALGO_FRAME_F32 : ALGO_DIRECT;
 
   unsigned *err_word = device_error_word();
   if (!err_word) return set_error(CCT_ECUDA, "device error word: symbol address lookup failed");

@@ -11,6 +11,13 @@
 // A thread holds 4 adjacent outputs x 8 output planes.  Summation order per
 // output matches the reference (per-row fma chain, row sum, plane sum), so
 // results are bit-identical to the FP32 CPU restatement.
+//
+// The same kernel without the reduce (REDUCE = false) serves the unfused
+// modes ProjectFrame / BackProjectFrame (CogFunctionAPI.scala:1370-1377,
+// 1425-1432), whose output plane b*F + k*N + c is input plane c of image b
+// correlated with one filter: each input plane's tile feeds the 16 filters
+// of the block and every result (per-row fma chain, row sum) is stored to
+// its own plane.
 #include "cct_internal.h"
 #include "sm100_util.cuh"
 #include "tile_common.cuh"
@@ -36,11 +43,11 @@ struct FrameTile {
   static constexpr int STAGE = TILE + FILT;
 };
 
-template <int R, int S, int DOWN>
+template <int R, int S, int DOWN, bool REDUCE>
 __global__ void __launch_bounds__(kThreads, 2)
     frame_f32_kernel(ConvGeom g, const float *__restrict__ x,
                      const float *__restrict__ f, float *__restrict__ y,
-                     int tiles_x, int tiles_y, int kblocks) {
+                     int tiles_x, int tiles_y, int kblocks, int tchunk) {
   grid_dependency_wait();  // launched with programmatic serialisation: nothing global before this
   using T = FrameTile<R, S, DOWN>;
   constexpr int E = (kU - 1) * DOWN + S;
@@ -54,7 +61,12 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int ty_i = bid % tiles_y;
   bid /= tiles_y;
   const int kb = bid % kblocks;
-  const int b = bid / kblocks;
+  bid /= kblocks;
+  // unfused modes: the input planes are split into chunks of tchunk, one per
+  // CTA (their outputs are independent); reduced modes: one chunk of all
+  const int nchunks = REDUCE ? 1 : (g.n + tchunk - 1) / tchunk;
+  const int t0 = REDUCE ? 0 : (bid % nchunks) * tchunk;
+  const int b = bid / nchunks;
   const int k0 = kb * kKB;
   const int kcount = min(kKB, g.groups - k0);
 
@@ -71,15 +83,16 @@ __global__ void __launch_bounds__(kThreads, 2)
   auto issue = [&](int t, int buf) {
     float *tile = smem + buf * T::STAGE;
     float *ft = tile + T::TILE;
-    const int ip = b * g.n + t;
+    const int ip = b * g.n + t0 + t;
     load_tile_async(tile, T::PITCH, T::IN_ROWS, T::IN_COLS, x + (size_t)ip * plane, g, org_r, org_c);
     for (int i = threadIdx.x; i < R * S * kKB; i += kThreads) {
       const int kk = i / (R * S), tap = i - kk * (R * S);
       const int r = tap / S, s = tap - r * S;
       const int src_tap = conv ? (R - 1 - r) * S + (S - 1 - s) : tap;
-      const int o = b * g.groups + k0 + kk;
+      // output plane of filter k0 + kk: b*K + k (reduced) or b*F + k*N + t
+      const int o = REDUCE ? b * g.groups + k0 + kk : b * g.pf + (k0 + kk) * g.n + t0 + t;
       int ipp, fp;
-      plane_pair(g, o, t, &ipp, &fp);
+      plane_pair(g, o, REDUCE ? t : 0, &ipp, &fp);
       const bool ok = kk < kcount;
       cp_async_f32(ft + tap * kKB + kk, ok ? f + (size_t)fp * (R * S) + src_tap : f, ok);
     }
@@ -96,9 +109,13 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
     for (int k = 0; k < kP; ++k) acc[u][k] = make_float2(0.0f, 0.0f);
 
+  const int nterms = REDUCE ? g.terms : min(tchunk, g.n - t0);
+  const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
+  const size_t opage = (size_t)g.OH * g.OW;
+  const int row = out_r0 + ty;
   issue(0, 0);
-  for (int t = 0; t < g.terms; ++t) {
-    if (t + 1 < g.terms) {
+  for (int t = 0; t < nterms; ++t) {
+    if (t + 1 < nterms) {
       issue(t + 1, (t + 1) & 1);
       cp_async_wait<1>();
     } else {
@@ -150,42 +167,70 @@ __global__ void __launch_bounds__(kThreads, 2)
 #pragma unroll
         for (int k = 0; k < kP; ++k) rs[u][k] = __fadd2_rn(rs[u][k], cs[u][k]);
     }
+    if (REDUCE) {
 #pragma unroll
-    for (int u = 0; u < kU; ++u)
+      for (int u = 0; u < kU; ++u)
 #pragma unroll
-      for (int k = 0; k < kP; ++k) acc[u][k] = (t == 0) ? rs[u][k] : __fadd2_rn(acc[u][k], rs[u][k]);
+        for (int k = 0; k < kP; ++k) acc[u][k] = (t == 0) ? rs[u][k] : __fadd2_rn(acc[u][k], rs[u][k]);
+    } else if (row < g.OH) {
+      // this input plane's result for each filter of the block: its own plane
+      const int col0 = out_c0 + tx * kU;
+      const bool vec = (g.OW & 3) == 0 && col0 + kU <= g.OW;
+#pragma unroll
+      for (int k = 0; k < kKT; ++k) {
+        const int kk = grp * kKT + k;
+        if (kk >= kcount) break;
+        float *ys = y + (size_t)(b * g.pf + (k0 + kk) * g.n + t0 + t) * opage + (size_t)row * g.OW;
+        float v[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const float a = (k & 1) ? rs[u][k >> 1].y : rs[u][k >> 1].x;
+          v[u] = relu ? fmaxf(a, 0.0f) : a;
+        }
+        if (vec) {
+          *reinterpret_cast<float4 *>(ys + col0) = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+#pragma unroll
+          for (int u = 0; u < kU; ++u)
+            if (col0 + u < g.OW) ys[col0 + u] = v[u];
+        }
+      }
+    }
     __syncthreads();
   }
 
-  const int row = out_r0 + ty;
-  if (row >= g.OH) return;
-  const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
-  const size_t opage = (size_t)g.OH * g.OW;
+  if constexpr (REDUCE) {
+    if (row >= g.OH) return;
 #pragma unroll
-  for (int k = 0; k < kKT; ++k) {
-    const int kk = grp * kKT + k;
-    if (kk >= kcount) break;
-    float *ys = y + (size_t)(b * g.groups + k0 + kk) * opage + (size_t)row * g.OW;
+    for (int k = 0; k < kKT; ++k) {
+      const int kk = grp * kKT + k;
+      if (kk >= kcount) break;
+      float *ys = y + (size_t)(b * g.groups + k0 + kk) * opage + (size_t)row * g.OW;
 #pragma unroll
-    for (int u = 0; u < kU; ++u) {
-      const int col = out_c0 + tx * kU + u;
-      const float a = (k & 1) ? acc[u][k >> 1].y : acc[u][k >> 1].x;
-      if (col < g.OW) ys[col] = relu ? fmaxf(a, 0.0f) : a;
+      for (int u = 0; u < kU; ++u) {
+        const int col = out_c0 + tx * kU + u;
+        const float a = (k & 1) ? acc[u][k >> 1].y : acc[u][k >> 1].x;
+        if (col < g.OW) ys[col] = relu ? fmaxf(a, 0.0f) : a;
+      }
     }
   }
 }
 
 template <int R, int S, int DOWN>
 int launch(const ConvGeom &g, const float *x, const float *f, float *y, cudaStream_t st) {
+  const bool reduce = g.mode == CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM || g.mode == CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM;
   using T = FrameTile<R, S, DOWN>;
   const int tiles_x = (g.OW + kTW - 1) / kTW, tiles_y = (g.OH + kTH - 1) / kTH;
   const int kblocks = (g.groups + kKB - 1) / kKB;
-  const long long blocks = (long long)tiles_x * tiles_y * kblocks * g.batch;
+  const int tchunk = reduce ? g.terms : 4;  // unfused: 4 input planes per CTA
+  const int nchunks = reduce ? 1 : (g.n + tchunk - 1) / tchunk;
+  const long long blocks = (long long)tiles_x * tiles_y * kblocks * nchunks * g.batch;
   if (blocks > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "frame grid too large");
   const size_t smem = 2 * sizeof(float) * T::STAGE;
   static_assert(2 * sizeof(float) * T::STAGE <= 48 * 1024, "frame stages exceed the default smem limit");
-  const int rc = launch_pdl(frame_f32_kernel<R, S, DOWN>, dim3((unsigned)blocks), dim3(kThreads), smem, st,
-                            "frame_f32_kernel launch", g, x, f, y, tiles_x, tiles_y, kblocks);
+  const int rc = launch_pdl(reduce ? frame_f32_kernel<R, S, DOWN, true> : frame_f32_kernel<R, S, DOWN, false>,
+                            dim3((unsigned)blocks), dim3(kThreads), smem, st, "frame_f32_kernel launch", g, x, f, y,
+                            tiles_x, tiles_y, kblocks, tchunk);
   if (!rc) count_launches(1);
   return rc;
 }
@@ -193,9 +238,10 @@ int launch(const ConvGeom &g, const float *x, const float *f, float *y, cudaStre
 }  // namespace
 
 bool frame_f32_supported(const ConvGeom &g) {
-  if (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM &&
-      g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
+  if (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM && g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM &&
+      g.mode != CCT_PROJECT_FRAME && g.mode != CCT_BACK_PROJECT_FRAME)
     return false;
+  if (g.up != 1) return false;
   if (g.R != g.S) return false;
   if (g.down != 1 && g.down != 2) return false;
   return g.R == 1 || g.R == 3 || g.R == 5 || g.R == 7 || g.R == 9;

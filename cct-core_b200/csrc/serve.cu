@@ -1,7 +1,8 @@
 // Request serving with continuous batching.
 //
-// A scheduler thread per server admits requests into an HBM arena as room
-// frees up, copies their inputs in, and packs the admitted ones into one
+// A scheduler thread per server admits requests as device memory for their
+// fields can be had from free HBM, copies their inputs in, and packs the
+// admitted ones into one
 // persistent launch per slot: `serve_batch_kernel` CTAs pull (request,
 // output plane, tile) work units from an atomic counter until the batch is
 // done, so requests of uneven sizes share one launch.  Each slot's launch
@@ -163,55 +164,102 @@ __global__ void __launch_bounds__(kThreads) serve_batch_kernel(const Batch *__re
 
 using Clock = std::chrono::steady_clock;
 
-// First-fit allocator over one device allocation (offsets 256-byte aligned).
-class Arena {
+// Device memory for admitted requests, claimed from free HBM in chunks.  A
+// request is admitted when a chunk has room for its fields (first fit,
+// 256-byte aligned blocks), or when the device's free memory, less the
+// reserve left for other work, can hold a new chunk for it.  With a cap, the
+// chunks together never exceed it.  Chunks are kept until the server is
+// destroyed: cudaFree synchronises the device, which the scheduler must not
+// do while launches are in flight.
+class Pool {
  public:
-  int init(size_t bytes) {
-    cap_ = bytes;
-    free_[0] = bytes;
-    return check_cuda(cudaMalloc(&base_, bytes), "cudaMalloc(server arena)");
+  void init(size_t cap, size_t reserve, size_t chunk) {
+    cap_ = cap;
+    reserve_ = reserve;
+    chunk_ = chunk;
   }
-  ~Arena() { cudaFree(base_); }
-  bool alloc(size_t bytes, size_t *off) {
+  ~Pool() {
+    for (auto &c : chunks_) cudaFree(c.base);
+  }
+  // Largest request the server can ever hold: the cap, or the device's
+  // total memory less the reserve.
+  size_t capacity() const {
+    if (cap_) return cap_;
+    size_t fr = 0, total = 0;
+    if (cudaMemGetInfo(&fr, &total) != cudaSuccess) return 0;
+    return total > reserve_ ? total - reserve_ : 0;
+  }
+  // A block of `bytes`, or nullptr when there is no room now.
+  char *alloc(size_t bytes) {
     bytes = (bytes + 255) & ~(size_t)255;
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= bytes) {
-        *off = it->first;
-        const size_t rem = it->second - bytes, start = it->first + bytes;
-        free_.erase(it);
-        if (rem) free_[start] = rem;
-        used_ += bytes;
-        peak_ = std::max(peak_, used_);
-        return true;
-      }
+    for (auto &c : chunks_) {
+      char *p = take(c, bytes);
+      if (p) return p;
     }
-    return false;
+    size_t size = std::max(bytes, chunk_);
+    if (cap_) {
+      if (held_ + bytes > cap_) return nullptr;
+      size = std::min(size, cap_ - held_);
+    }
+    size_t fr = 0, total = 0;
+    if (cudaMemGetInfo(&fr, &total) != cudaSuccess) return nullptr;
+    if (fr < reserve_ + bytes) return nullptr;
+    size = std::min(size, fr - reserve_);
+    size = (size + 255) & ~(size_t)255;
+    Chunk c;
+    if (cudaMalloc(&c.base, size) != cudaSuccess) {
+      cudaGetLastError();  // out of memory now: wait for releases
+      return nullptr;
+    }
+    c.cap = size;
+    c.free[0] = size;
+    held_ += size;
+    chunks_.push_back(std::move(c));
+    return take(chunks_.back(), bytes);
   }
-  void release(size_t off, size_t bytes) {
+  void release(char *p, size_t bytes) {
     bytes = (bytes + 255) & ~(size_t)255;
-    used_ -= bytes;
-    auto it = free_.emplace(off, bytes).first;
-    auto next = std::next(it);
-    if (next != free_.end() && it->first + it->second == next->first) {
-      it->second += next->second;
-      free_.erase(next);
-    }
-    if (it != free_.begin()) {
-      auto prev = std::prev(it);
-      if (prev->first + prev->second == it->first) {
-        prev->second += it->second;
-        free_.erase(it);
+    for (auto &c : chunks_) {
+      if (p < c.base || p >= c.base + c.cap) continue;
+      used_ -= bytes;
+      auto it = c.free.emplace((size_t)(p - c.base), bytes).first;
+      auto next = std::next(it);
+      if (next != c.free.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        c.free.erase(next);
       }
+      if (it != c.free.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+          prev->second += it->second;
+          c.free.erase(it);
+        }
+      }
+      return;
     }
   }
-  float *at(size_t off) const { return reinterpret_cast<float *>(static_cast<char *>(base_) + off); }
-  size_t capacity() const { return cap_; }
   size_t peak() const { return peak_; }
 
  private:
-  void *base_ = nullptr;
-  size_t cap_ = 0, used_ = 0, peak_ = 0;
-  std::map<size_t, size_t> free_;
+  struct Chunk {
+    char *base = nullptr;
+    size_t cap = 0;
+    std::map<size_t, size_t> free;  // offset -> bytes
+  };
+  char *take(Chunk &c, size_t bytes) {
+    for (auto it = c.free.begin(); it != c.free.end(); ++it) {
+      if (it->second < bytes) continue;
+      const size_t off = it->first, rem = it->second - bytes;
+      c.free.erase(it);
+      if (rem) c.free[off + bytes] = rem;
+      used_ += bytes;
+      peak_ = std::max(peak_, used_);
+      return c.base + off;
+    }
+    return nullptr;
+  }
+  std::vector<Chunk> chunks_;
+  size_t cap_ = 0, reserve_ = 0, chunk_ = 0, held_ = 0, used_ = 0, peak_ = 0;
 };
 
 struct Req {
@@ -220,7 +268,8 @@ struct Req {
   ConvGeom g{};
   bool batchable = false;
   size_t x_elems = 0, f_elems = 0, y_elems = 0;
-  size_t off = 0, bytes = 0;  // arena block: x, then f (host filters), then y
+  char *dev = nullptr;  // device block: x, then f (host filters), then y
+  size_t bytes = 0;
   size_t off_f = 0, off_y = 0;  // offsets of f and y inside the block (256-byte aligned)
   Clock::time_point t_submit;
   double latency_us = 0.0;
@@ -254,7 +303,7 @@ struct cct_server {
   cct_server_config cfg{};
   int device = 0;
   int grid = 0;
-  Arena arena;
+  Pool pool;
   std::vector<std::unique_ptr<Slot>> slots;
   std::vector<float *> filters;
   std::vector<size_t> filter_elems;
@@ -272,7 +321,7 @@ struct cct_server {
 
   // scheduler-only state
   std::deque<ReqPtr> waiting;   // not yet admitted (arrival order)
-  std::deque<ReqPtr> admitted;  // in the arena, not yet launched
+  std::deque<ReqPtr> admitted;  // holding device memory, not yet launched
   std::set<cct_graph *> busy_graphs;
 
   std::atomic<uint64_t> completed{0}, batches{0}, solo{0};
@@ -298,7 +347,7 @@ int launch_solo(cct_server *s, Req &q, const float *x, const float *f, float *y,
 }
 
 const float *filter_ptr(cct_server *s, const Req &q) {
-  return q.r.filter ? s->arena.at(q.off + q.off_f) : s->filters[q.r.filter_id];
+  return q.r.filter ? reinterpret_cast<float *>(q.dev + q.off_f) : s->filters[q.r.filter_id];
 }
 
 int copy_in(cct_server *s, Req &q, cudaStream_t st) {
@@ -309,11 +358,11 @@ int copy_in(cct_server *s, Req &q, cudaStream_t st) {
     if (rc) return rc;
     return check_cuda(cudaMemcpyAsync(in, q.r.image, n * sizeof(float), cudaMemcpyHostToDevice, st), "H2D request");
   }
-  int rc = check_cuda(cudaMemcpyAsync(s->arena.at(q.off), q.r.image, q.x_elems * sizeof(float),
+  int rc = check_cuda(cudaMemcpyAsync(q.dev, q.r.image, q.x_elems * sizeof(float),
                                       cudaMemcpyHostToDevice, st),
                       "H2D request image");
   if (!rc && q.r.filter)
-    rc = check_cuda(cudaMemcpyAsync(s->arena.at(q.off + q.off_f), q.r.filter,
+    rc = check_cuda(cudaMemcpyAsync(q.dev + q.off_f, q.r.filter,
                                     q.f_elems * sizeof(float), cudaMemcpyHostToDevice, st),
                     "H2D request filter");
   return rc;
@@ -329,16 +378,16 @@ int copy_out(cct_server *s, Req &q, cudaStream_t st) {
     if (rc) return rc;
     return check_cuda(cudaMemcpyAsync(q.r.out, out, n * sizeof(float), cudaMemcpyDeviceToHost, st), "D2H request");
   }
-  return check_cuda(cudaMemcpyAsync(q.r.out, s->arena.at(q.off + q.off_y), q.y_elems * sizeof(float),
+  return check_cuda(cudaMemcpyAsync(q.r.out, q.dev + q.off_y, q.y_elems * sizeof(float),
                                     cudaMemcpyDeviceToHost, st),
                     "D2H request output");
 }
 
-float *out_ptr(cct_server *s, const Req &q) { return s->arena.at(q.off + q.off_y); }
+float *out_ptr(cct_server *, const Req &q) { return reinterpret_cast<float *>(q.dev + q.off_y); }
 
 void fill_item(cct_server *s, const Req &q, Item *it) {
   const ConvGeom &g = q.g;
-  it->x = s->arena.at(q.off);
+  it->x = reinterpret_cast<float *>(q.dev);
   it->f = filter_ptr(s, q);
   it->y = out_ptr(s, q);
   it->H = g.H;
@@ -366,7 +415,7 @@ void finish(cct_server *s, Req &q, int status, Clock::time_point t) {
   q.status = status;
   if (status != CCT_OK) q.msg = cct_last_error_string();
   q.latency_us = std::chrono::duration<double, std::micro>(t - q.t_submit).count();
-  if (q.r.kind == CCT_SERVE_CONV) s->arena.release(q.off, q.bytes);
+  if (q.r.kind == CCT_SERVE_CONV) s->pool.release(q.dev, q.bytes);
   q.done = true;
   s->completed.fetch_add(1, std::memory_order_relaxed);
 }
@@ -394,12 +443,13 @@ bool retire(cct_server *s) {
   return any;
 }
 
-// Scheduler: admit waiting requests into the arena, in arrival order.
+// Scheduler: admit waiting requests, in arrival order, while device memory
+// for their fields can be had.
 bool admit(cct_server *s) {
   bool any = false;
   while (!s->waiting.empty()) {
     ReqPtr q = s->waiting.front();
-    if (q->r.kind == CCT_SERVE_CONV && !s->arena.alloc(q->bytes, &q->off)) break;
+    if (q->r.kind == CCT_SERVE_CONV && !(q->dev = s->pool.alloc(q->bytes))) break;
     s->waiting.pop_front();
     s->admitted.push_back(q);
     any = true;
@@ -455,7 +505,7 @@ bool launch(cct_server *s) {
       it.first = b.total;
       b.total += (long long)it.K * it.tiles_x * it.tiles_y;
     } else {
-      rc = launch_solo(s, *q, s->arena.at(q->off), q->r.kind == CCT_SERVE_CONV ? filter_ptr(s, *q) : nullptr,
+      rc = launch_solo(s, *q, reinterpret_cast<float *>(q->dev), q->r.kind == CCT_SERVE_CONV ? filter_ptr(s, *q) : nullptr,
                        q->r.kind == CCT_SERVE_CONV ? out_ptr(s, *q) : nullptr, sl.st);
       s->solo.fetch_add(1, std::memory_order_relaxed);
     }
@@ -545,10 +595,10 @@ int autotune(cct_server *s) {
   Slot &sl = *s->slots[0];
   const int H = 96, W = 96, C = 4, K = 16, items = 8;
   const size_t x_el = (size_t)C * H * W, f_el = (size_t)K * C * kMaxR * kMaxR, y_el = (size_t)K * H * W;
-  size_t off = 0;
   const size_t bytes = (x_el + f_el + y_el) * sizeof(float);
-  if (!s->arena.alloc(bytes, &off)) return CCT_OK;  // arena too small to tune: keep defaults
-  float *x = s->arena.at(off), *f = x + x_el, *y = f + f_el;
+  char *blk = s->pool.alloc(bytes);
+  if (!blk) return CCT_OK;  // no device memory to tune with: keep defaults
+  float *x = reinterpret_cast<float *>(blk), *f = x + x_el, *y = f + f_el;
   cudaMemsetAsync(x, 0, bytes, sl.st);
   cudaEvent_t a, b;
   cudaEventCreate(&a);
@@ -617,7 +667,7 @@ int autotune(cct_server *s) {
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
-  s->arena.release(off, bytes);
+  s->pool.release(blk, bytes);
   return check_cuda(cudaStreamSynchronize(sl.st), "server autotune");
 }
 
@@ -631,7 +681,8 @@ void cct_server_config_init(cct_server_config *cfg) {
   cfg->struct_size = sizeof(*cfg);
   cfg->slots = 3;
   cfg->max_batch = 64;
-  cfg->arena_bytes = 8ull << 30;
+  cfg->arena_bytes = 0;                 // no cap: admission by free HBM
+  cfg->hbm_reserve_bytes = 2ull << 30;  // left free for other work on the device
 }
 
 void cct_serve_request_init(cct_serve_request *req) {
@@ -653,7 +704,8 @@ int cct_server_create(const cct_server_config *cfg, cct_server **out) {
                        sizeof(cct_server_config));
     if (cfg->slots) c.slots = cfg->slots;
     if (cfg->max_batch) c.max_batch = cfg->max_batch;
-    if (cfg->arena_bytes) c.arena_bytes = cfg->arena_bytes;
+    c.arena_bytes = cfg->arena_bytes;
+    if (cfg->hbm_reserve_bytes) c.hbm_reserve_bytes = cfg->hbm_reserve_bytes;
     c.flags = cfg->flags;
   }
   if (c.slots < 1 || c.slots > 8) return set_error(CCT_EINVAL, "slots must be 1..8, got %d", c.slots);
@@ -673,7 +725,8 @@ int cct_server_create(const cct_server_config *cfg, cct_server **out) {
                     "occupancy(serve)");
   if (rc) return rc;
   s->grid = sms * std::max(per_sm, 1);
-  rc = s->arena.init(c.arena_bytes);
+  // chunks of 1 GiB (or the cap, if smaller), a larger request gets a chunk of its own
+  s->pool.init(c.arena_bytes, c.hbm_reserve_bytes, std::min<size_t>(c.arena_bytes ? c.arena_bytes : ~(size_t)0, (size_t)1 << 30));
   for (int i = 0; i < c.slots && !rc; ++i) {
     s->slots.emplace_back(new Slot);
     rc = capture_slot(s.get(), *s->slots.back());
@@ -767,9 +820,10 @@ int cct_server_submit(cct_server *s, const cct_serve_request *req, uint64_t *tic
     q->off_f = al(q->x_elems * sizeof(float));
     q->off_y = q->off_f + (req->filter ? al(q->f_elems * sizeof(float)) : 0);
     q->bytes = q->off_y + al(q->y_elems * sizeof(float));
-    if (q->bytes > s->arena.capacity())
+    const size_t cap = s->pool.capacity();
+    if (q->bytes > cap)
       return set_error(CCT_EINVAL, "request needs %zu bytes of device memory, the server's arena holds %zu",
-                       q->bytes, s->arena.capacity());
+                       q->bytes, cap);
     q->flops = 2.0 * q->y_elems * g.R * g.S * g.terms;
     q->batchable = g.border == CCT_BORDER_ZERO && g.down == 1 && g.up == 1 && g.R == g.S && (g.R & 1) &&
                    g.R <= kMaxR && g.pin >= 1 && q->flops < s->solo_flops;
@@ -843,7 +897,7 @@ int cct_server_stats(const cct_server *s, uint64_t *completed, uint64_t *batches
   if (completed) *completed = s->completed.load();
   if (batches) *batches = s->batches.load();
   if (solo) *solo = s->solo.load();
-  if (peak_arena_bytes) *peak_arena_bytes = s->arena.peak();
+  if (peak_arena_bytes) *peak_arena_bytes = s->pool.peak();
   return CCT_OK;
 }
 

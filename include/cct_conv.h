@@ -299,10 +299,13 @@ int cct_graph_restore(const uint32_t *words, size_t n_words, cct_graph **graph);
 
 /* ---- request serving (continuous batching) ------------------------------ */
 /* No counterpart in the reference, whose ComputeGraphs are stepped by one
- * caller at a time.  A server owns one GPU's share of HBM (an arena of
- * `arena_bytes`) and a scheduler thread.  Requests (a convolution, or a step
- * of a resident cct_graph) arrive from any thread; each is admitted when
- * the arena has room for its fields, its inputs are copied in, and admitted
+ * caller at a time.  A server serves one GPU with a scheduler thread.
+ * Requests (a convolution, or a step of a resident cct_graph) arrive from
+ * any thread; each is admitted when device memory for its fields can be
+ * had: from the server's chunks of device memory, or from the device's free
+ * HBM (cudaMemGetInfo) less `hbm_reserve_bytes`, claimed as a new chunk;
+ * `arena_bytes`, if nonzero, caps what the server holds.  Its inputs are
+ * copied in, and admitted
  * requests are batched into one persistent kernel launch (a captured CUDA
  * graph per launch slot) whose CTAs pull tiles of every request in the
  * batch.  Up to `slots` launches are in flight on their own streams, so
@@ -326,7 +329,8 @@ typedef struct cct_server_config {
   int32_t slots;        /* launches in flight (1..8; 0 = 3) */
   int32_t max_batch;    /* requests per launch (1..256; 0 = 64) */
   int32_t flags;
-  uint64_t arena_bytes; /* HBM reserved for admitted requests (0 = 8 GiB) */
+  uint64_t arena_bytes; /* cap on the HBM the server holds (0 = none: admission by free HBM) */
+  uint64_t hbm_reserve_bytes; /* free HBM the server leaves to other work (0 = 2 GiB) */
 } cct_server_config;
 typedef struct cct_serve_request {
   int32_t struct_size;  /* sizeof(cct_serve_request) */
@@ -347,7 +351,8 @@ int cct_server_create(const cct_server_config *cfg, cct_server **out);
 int cct_server_destroy(cct_server *server);
 /* A filter bank kept resident on the device; requests name it by id. */
 int cct_server_add_filter(cct_server *server, const float *host_filter, size_t elems, int32_t *id);
-/* Queues a request (CCT_EINVAL if it can never fit the arena or is malformed). */
+/* Queues a request (CCT_EINVAL if it can never fit: larger than the cap, or
+ * than the device's memory less the reserve; or malformed). */
 int cct_server_submit(cct_server *server, const cct_serve_request *req, uint64_t *ticket);
 /* CCT_OK once the request's output is in host memory; CCT_ETIMEOUT after
  * timeout_ms (< 0: no limit); the request's own error status otherwise.

@@ -133,7 +133,8 @@ def test_server_and_graph_need_a_device():
     cfg = _lib.ServerConfig()
     _lib.LIB.cct_server_config_init(ctypes.byref(cfg))
     assert cfg.struct_size == ctypes.sizeof(_lib.ServerConfig)
-    assert cfg.slots == 3 and cfg.max_batch == 64 and cfg.arena_bytes == 8 << 30
+    assert cfg.slots == 3 and cfg.max_batch == 64 and cfg.arena_bytes == 0  # admission by free HBM
+    assert cfg.hbm_reserve_bytes == 2 << 30
     h = ctypes.c_void_p()
     import torch
     if torch.cuda.is_available():

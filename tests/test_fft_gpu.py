@@ -151,6 +151,45 @@ def test_fft_when_best_takes_fft_for_large_filters_only():
         p.close()
 
 
+def _launch_us(plan, x, f, y, reps=10):
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        plan.run(x.data_ptr(), f.data_ptr(), y.data_ptr(), st)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        plan.run(x.data_ptr(), f.data_ptr(), y.data_ptr(), st)
+    b.record()
+    b.synchronize()
+    return a.elapsed_time(b) * 1e3 / reps
+
+
+@pytest.mark.parametrize("R", [15, 31])
+def test_fft_when_best_takes_the_measured_faster_path(R):
+    """UseFFTWhenBest on a 1024x1024 field with a 15x15 or 31x31 filter (where
+    the modelled costs are close, so the plan times both paths on the
+    device): the plan takes the path that is faster here, or one within 20%
+    of it (the FFT must win by 1.2x to be taken over the exact direct path)."""
+    n = 1024
+    auto = _lib.Plan(_desc(n, n, R, R, 0, 0, _lib.BORDER_ZERO, _lib.CONVOLUTION, algo=_lib.ALGO_AUTO))
+    direct = _lib.Plan(_desc(n, n, R, R, 0, 0, _lib.BORDER_ZERO, _lib.CONVOLUTION, algo=_lib.ALGO_DIRECT))
+    fft = _lib.Plan(_desc(n, n, R, R, 0, 0, _lib.BORDER_ZERO, _lib.CONVOLUTION, algo=_lib.ALGO_FFT))
+    assert fft.algo == _lib.PLAN_FFT and direct.algo != _lib.PLAN_FFT
+    x = torch.rand((n, n), device="cuda")
+    f = torch.rand((R, R), device="cuda")
+    y = torch.empty((n, n), device="cuda")
+    fh = f.cpu().numpy()
+    fft.set_static_filter(fh.ctypes.data)  # the triage times the FFT with a static filter
+    t_direct = _launch_us(direct, x, f, y)
+    t_fft = min(_launch_us(fft, x, f, y), _launch_us(fft, x, f, y))
+    faster = _lib.PLAN_FFT if t_fft < t_direct else direct.algo
+    slower_ok = max(t_direct, t_fft) <= 1.2 * min(t_direct, t_fft)
+    print(f"{R}x{R} on {n}^2: direct {t_direct:.1f} us, fft {t_fft:.1f} us, auto took algo {auto.algo}")
+    assert auto.algo == faster or slower_ok, (t_direct, t_fft, auto.algo)
+    for p in (auto, direct, fft):
+        p.close()
+
+
 @pytest.mark.parametrize("case", ["valid", "full", "downsample", "upsample", "frame"])
 def test_fft_always_falls_back_where_the_fft_cannot_go(case):
     """UseFFTAlways on a form the FFT generator does not take runs the direct

@@ -128,7 +128,22 @@ MODE_CASES = [
     (O.BACKPROJECT_REDUCE, 8, 32, 2, 5, O.CYCLIC, O.DOWN, 2),
     (O.BACKPROJECT_REDUCE, 34, 17 * 3, 2, 3, O.ZERO, O.NOSAMPLE, 1),
     (O.BACKPROJECT_REDUCE, 4, 12, 1, 5, O.FULL, O.UP, 3),
+    # unfused frame modes with several 16-filter blocks (the FP32 frame kernel
+    # without its reduce: every input plane's result to its own output plane)
+    (O.PROJECT, 2 * 5, 37 * 5, 2, 7, O.CLAMP, O.NOSAMPLE, 1),
+    (O.BACKPROJECT, 2 * 6, 6 * 20, 2, 3, O.CYCLIC, O.DOWN, 2),
 ]
+
+
+@pytest.mark.parametrize("mode", [O.PROJECT, O.BACKPROJECT])
+def test_unfused_frame_modes_take_the_frame_kernel(mode):
+    od = O.make_desc(32, 40, 5, 5, planes=2 * 8, f_planes=40 * 8, batch=2, border=O.ZERO, orient=O.XCORR,
+                     mode=mode)
+    x = np.random.default_rng(4).normal(size=(16, 32, 40)).astype(np.float32)
+    f = np.random.default_rng(5).normal(size=(320, 5, 5)).astype(np.float32)
+    y, algo = gpu_conv(od, x, f)
+    assert algo == _lib.PLAN_FRAME_F32
+    assert bitwise_equal(y, O.conv(od, x, f))
 
 
 @pytest.mark.parametrize("mode,planes,fplanes,batch,fs,border,samp,step", MODE_CASES)

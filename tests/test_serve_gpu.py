@@ -1,9 +1,9 @@
 """Request serving: continuous batching gives every request the result it gets
 alone, bit for bit, and the FP32 oracle's result.
 
-Requests of uneven sizes (fields 32-200 on a side, 3x3 to 9x9 filters, 1-16
-input planes, 1 or 16 filters) arrive as a burst; the server admits them into
-its arena as room frees up and batches them into persistent launches.  Each
+Requests of uneven sizes (fields 32-1024 on a side, 3x3 to 9x9 filters, 1-64
+input planes, 1-64 filters) arrive as a burst; the server admits them as
+device memory frees up and batches them into persistent launches.  Each
 result is compared with the same request served alone (per-call dispatch,
 one request at a time) and with the FP32 oracle.
 """
@@ -75,12 +75,12 @@ def _serve_all(server, reqs):
 
 def test_results_alone_and_in_the_mix_are_identical_and_exact():
     mix = Mix(48, seed=1)
-    alone = Server(per_call=True, arena_bytes=1 << 30)
+    alone = Server(per_call=True)
     reqs_a, outs_a = mix.requests()
     _serve_all(alone, reqs_a)
     alone.close()
 
-    server = Server(slots=3, max_batch=16, arena_bytes=1 << 30)
+    server = Server(slots=3, max_batch=16)
     reqs_m, outs_m = mix.requests()
     _serve_all(server, reqs_m)
     st = server.stats()
@@ -90,9 +90,51 @@ def test_results_alone_and_in_the_mix_are_identical_and_exact():
     for i, ((side, R, C, K), x, f) in enumerate(zip(mix.specs, mix.x, mix.f)):
         a, m = outs_a[i].numpy(), outs_m[i].numpy()
         assert np.array_equal(a.view(np.uint32), m.view(np.uint32)), (i, mix.specs[i])
-        if i % 4 == 0:  # the oracle is slow on the largest requests: a quarter of them
-            ref = _oracle(side, R, C, K, x.numpy(), f.numpy())
-            assert np.array_equal(m.reshape(ref.shape).view(np.uint32), ref.view(np.uint32)), i
+        ref = _oracle(side, R, C, K, x.numpy(), f.numpy())
+        assert np.array_equal(m.reshape(ref.shape).view(np.uint32), ref.view(np.uint32)), i
+
+
+# Requests spanning the serving stream's ranges (side 32-1024, 3x3-9x9, 1-64
+# planes, 1-64 filters): the largest run alone on their own plan, the small
+# ones share batch launches.  (side, R, planes, filters)
+WIDE = [(1024, 9, 1, 1), (1024, 3, 64, 1), (1024, 5, 4, 16), (724, 7, 16, 1), (512, 3, 64, 64),
+        (362, 9, 16, 16), (256, 5, 64, 16), (181, 3, 4, 64), (128, 9, 64, 1), (90, 7, 16, 64),
+        (64, 5, 1, 16), (45, 3, 64, 64), (32, 9, 4, 1), (32, 3, 1, 64), (600, 5, 1, 64),
+        (100, 3, 16, 16)]
+
+
+class SpecMix(Mix):
+    def __init__(self, specs, seed):
+        rng = np.random.default_rng(seed)
+        self.specs, self.x, self.f = [], [], []
+        for side, R, C, K in specs:
+            self.specs.append((side, R, C, K))
+            self.x.append(torch.from_numpy(rng.uniform(-1, 1, (C, side, side)).astype(np.float32)).pin_memory())
+            fp = 1 if K == 1 else K * C
+            self.f.append(torch.from_numpy(rng.uniform(-1, 1, (fp, R, R)).astype(np.float32)).pin_memory())
+
+
+def test_serving_ranges_alone_and_in_the_mix_match_the_oracle():
+    """Every request of a mix spanning the stream's full size ranges: served
+    alone, served in the mix (batched and solo routes both taken), and the
+    FP32 oracle agree bit for bit."""
+    mix = SpecMix(WIDE, seed=9)
+    alone = Server(per_call=True)
+    reqs_a, outs_a = mix.requests()
+    _serve_all(alone, reqs_a)
+    alone.close()
+    server = Server(slots=3, max_batch=16)
+    reqs_m, outs_m = mix.requests()
+    _serve_all(server, reqs_m)
+    st = server.stats()
+    server.close()
+    assert st["completed"] == len(reqs_m)
+    assert st["solo"] > 0 and st["batches"] > 0, st  # both routes taken
+    for i, ((side, R, C, K), x, f) in enumerate(zip(mix.specs, mix.x, mix.f)):
+        a, m = outs_a[i].numpy(), outs_m[i].numpy()
+        assert np.array_equal(a.view(np.uint32), m.view(np.uint32)), (i, mix.specs[i])
+        ref = _oracle(side, R, C, K, x.numpy(), f.numpy())
+        assert np.array_equal(m.reshape(ref.shape).view(np.uint32), ref.view(np.uint32)), (i, mix.specs[i])
 
 
 def test_admission_waits_for_arena_room():
@@ -108,6 +150,32 @@ def test_admission_waits_for_arena_room():
     for i, ((side, R, C, K), x, f) in enumerate(zip(mix.specs, mix.x, mix.f)):
         ref = _oracle(side, R, C, K, x.numpy(), f.numpy())
         assert np.array_equal(outs[i].numpy().reshape(ref.shape).view(np.uint32), ref.view(np.uint32)), i
+
+
+def test_admission_by_free_hbm():
+    """With no cap, a server claims device memory from the device's free HBM
+    less its reserve: leaving all but 128 MiB of the free memory to other
+    work, it still serves every request (within those 128 MiB); a request
+    larger than the device's memory less the reserve is rejected at once."""
+    free, total = torch.cuda.mem_get_info()
+    server = Server(slots=2, max_batch=8, hbm_reserve_bytes=free - (128 << 20))
+    mix = Mix(12, seed=3, max_side=128)
+    reqs, outs = mix.requests()
+    _serve_all(server, reqs)
+    st = server.stats()
+    server.close()
+    assert st["completed"] == len(reqs)
+    assert st["peak_arena_bytes"] <= 128 << 20
+    for i, ((side, R, C, K), x, f) in enumerate(zip(mix.specs, mix.x, mix.f)):
+        ref = _oracle(side, R, C, K, x.numpy(), f.numpy())
+        assert np.array_equal(outs[i].numpy().reshape(ref.shape).view(np.uint32), ref.view(np.uint32)), i
+    server = Server(hbm_reserve_bytes=total - (64 << 20))
+    x = torch.zeros((16, 1024, 1024)).pin_memory()
+    y = torch.zeros((16, 1024, 1024)).pin_memory()
+    f = torch.zeros((1, 3, 3)).pin_memory()
+    with pytest.raises(_lib.CctError, match="arena holds"):  # 128 MiB of fields
+        server.submit(conv_request(_desc(1024, 3, 16, 1), x.data_ptr(), y.data_ptr(), f.data_ptr()))
+    server.close()
 
 
 def test_resident_filters_and_rejections():
@@ -168,7 +236,7 @@ def test_graph_step_requests_match_stepping_the_graph():
 def test_replay_reports_latencies():
     mix = Mix(40, seed=6, max_side=128)
     reqs, outs = mix.requests()
-    server = Server(slots=3, max_batch=16, arena_bytes=1 << 30)
+    server = Server(slots=3, max_batch=16)
     arrivals = np.cumsum(np.random.default_rng(7).exponential(1 / 2000.0, len(reqs)))
     lat = server.replay(reqs, arrivals)
     server.close()

@@ -77,6 +77,7 @@ constexpr uint32_t kAccCols = 256;  // one accumulator (N <= 256 fp32 columns)
 constexpr int kXchPitch = 17;
 constexpr int kXchFloats = 32 * kXchPitch;
 constexpr size_t kXchBytes = 4 * 2 * kXchFloats * sizeof(float);
+constexpr size_t kXchBytesPair = 2 * 6 * kXchFloats * sizeof(float);
 
 // Filter chunk row blocks (64 rows each) and the MMAs over them.
 // Block contents: -1 zero, else the split term (0 hi, 1 mid / lo for 2 terms, 2 lo).
@@ -85,16 +86,28 @@ __host__ __device__ constexpr int block_term(int terms, int blk) {
                     : (blk == 0 || blk == 3 || blk == 5 ? -1             // Z Fh Fm Z Fl Z Fm
                                                         : (blk == 1 ? 0 : blk == 2 ? 1 : blk == 4 ? 2 : 1));
 }
-template <int TERMS>
+// Paired taps (banks of at most 32 filters): a chunk of 32-row blocks
+// [Fh_a Fl_a Fh_b Fl_b 0 Fh_a 0 Fh_b] for taps a and b = a + 1 of one filter
+// row; -1 zero, else (term, which tap).
+__host__ __device__ constexpr int pair_block_term(int blk) { return blk == 4 || blk == 6 ? -1 : (blk & 1) && blk < 4 ? 1 : 0; }
+__host__ __device__ constexpr int pair_block_tap(int blk) { return blk == 2 || blk == 3 || blk == 7 ? 1 : 0; }
+template <int TERMS, bool PAIR>
 struct MmaList;
 template <>
-struct MmaList<2> {
+struct MmaList<2, false> {
   static constexpr int n = 2;
   __device__ static int arow(int m) { return m == 0 ? 64 : 0; }  // [Fh; Fl], [0; Fh]
   __device__ static int bterm(int m) { return m; }               // Xh, Xl
 };
 template <>
-struct MmaList<3> {
+struct MmaList<2, true> {
+  static constexpr int n = 2;
+  // [Fh_a; Fl_a; Fh_b; Fl_b] x Xh, [0; Fh_a; 0; Fh_b] x Xl, at tap a's offset
+  __device__ static int arow(int m) { return m == 0 ? 0 : 128; }
+  __device__ static int bterm(int m) { return m; }
+};
+template <>
+struct MmaList<3, false> {
   static constexpr int n = 5;
   // [Fh; Fm] x Xh, [0; Fh] x Xm, [0; Fh] x Xl, [0; Fl] x Xh, [0; Fm] x Xm
   __device__ static int arow(int m) { return m == 0 ? 64 : m == 3 ? 192 : m == 4 ? 320 : 0; }
@@ -129,7 +142,7 @@ __device__ __forceinline__ bool border_map(const ConvGeom &g, int iy, int ix, in
 }
 
 struct Item {
-  int b, band, tile, nb;
+  int b, ph, band, tile, nb;
 };
 __device__ __forceinline__ Item decode(const BankParams &p, int i) {
   Item it;
@@ -138,8 +151,35 @@ __device__ __forceinline__ Item decode(const BankParams &p, int i) {
   it.tile = rest % p.tiles_band;
   rest /= p.tiles_band;
   it.band = rest % p.nbands;
-  it.b = rest / p.nbands;
+  rest /= p.nbands;
+  it.ph = rest % p.nph_out;
+  it.b = rest / p.nph_out;
   return it;
+}
+
+// Reduction units of a work item: ts taps per filter row of its (sub-)filter,
+// nu units, nst stages per plane block, and the first packed chunk of its
+// filter block.  Every role derives its loop bounds from here.
+struct ItemUnits {
+  int ts, nu, nst;
+  size_t chunk0;
+};
+template <bool PAIR>
+__device__ __forceinline__ ItemUnits item_units(const BankParams &p, const Item &it) {
+  ItemUnits r;
+  int rows;
+  if (p.up > 1) {
+    const int rho = it.ph / p.up;
+    rows = p.up_rq[rho];
+    r.ts = p.up_sq[it.ph - rho * p.up];
+  } else {
+    rows = p.g.R;
+    r.ts = p.g.S;
+  }
+  r.nu = rows * (PAIR ? (r.ts + 1) / 2 : r.ts);
+  r.nst = (r.nu + p.T - 1) / p.T;
+  r.chunk0 = (size_t)p.up_choff[it.ph] + (size_t)it.nb * p.NCB * r.nu;
+  return r;
 }
 
 // Split 8*KG planes of one halo position into bf16 terms and store them as
@@ -174,11 +214,13 @@ __device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, 
   }
 }
 
-template <int TERMS>
+template <int TERMS, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_constant__ BankParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ Bars bars;
-  __shared__ float xch[4 * 2 * kXchFloats];  // epilogue exchange: 4 warp pairs x 2 buffers
+  // epilogue exchange: 4 warp pairs x 2 buffers, or (paired taps) 2 groups of
+  // 4 warps x 3 parts x 2 buffers
+  __shared__ float xch[(PAIR ? 12 : 8) * kXchFloats];
   const ConvGeom &g = p.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t *halo = smem;                                 // 2 x halo_bytes
@@ -210,8 +252,6 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
   allow_dependent_launch();
 
   volatile int *abort_flag = &bars.abort_flag;
-  const int tstages = p.NCB * p.nst;                            // stages per tile
-  const int nseg = (tstages + p.seg_stages - 1) / p.seg_stages;  // accumulation segments per tile
 
   if (warp < kConvWarps) {
     // ------------------------------------------------------------ converters
@@ -222,8 +262,11 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     bool failed = false;
     for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
       const Item it = decode(p, i);
-      const int p0 = it.tile * p.N;
-      const int col0 = it.band * p.BW + p.sc_min;  // strided input column of halo column 0
+      const int p0 = it.tile * p.tile_adv;
+      // strided input row / column of halo position 0
+      const int rho = it.ph / p.up, kap = it.ph - rho * p.up;
+      const int row0 = p.up > 1 ? p.up_sr[rho] : p.sr_min;
+      const int col0 = it.band * p.BW + (p.up > 1 ? p.up_sc[kap] : p.sc_min);
       const float *xb = p.x + (size_t)it.b * g.n * plane;
       for (int cb = 0; cb < p.NCB; ++cb, ++hb) {
         const int buf = hb & 1;
@@ -239,7 +282,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           for (int q = threadIdx.x; q < p.L; q += kConvThreads) {
             const int G = p0 + q;
             const int Y = G / p.P, X = G - Y * p.P;
-            const int iy = g.down * (Y + p.sr_min) + p.phase_r[ph];
+            const int iy = g.down * (Y + row0) + p.phase_r[ph];
             const int ix = g.down * (col0 + X) + p.phase_c[ph];
             int ry, rx;
             const bool in = border_map(g, iy, ix, ry, rx);
@@ -263,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     if (failed) *abort_flag = 1;
   } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
-    using ML = MmaList<TERMS>;
+    using ML = MmaList<TERMS, PAIR>;
     const uint32_t idesc = idesc_bf16_f32(128, p.N);
     // Operand descriptors are a template (layout, strides) plus the address
     // in 16-byte units; shared-memory addresses stay below 256 KB, so the
@@ -277,6 +320,9 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     uint32_t q = 0, hb = 0, u = 0;
     bool failed = false;
     for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
+      const ItemUnits iu = item_units<PAIR>(p, decode(p, i));
+      const int hs = PAIR ? (iu.ts + 1) / 2 : iu.ts;  // units per filter row
+      const int tstages = p.NCB * iu.nst;
       int seg_left = 0, done = 0, bi = 0;
       bool first = false;
       for (int cb = 0; cb < p.NCB && !failed; ++cb, ++hb) {
@@ -285,7 +331,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         if (failed) break;
         tc_fence_after();
         const uint64_t hdesc = b_tmpl + halo0 + (uint32_t)buf * (p.halo_bytes >> 4);
-        for (int st = 0; st < p.nst; ++st, ++q) {
+        for (int st = 0; st < iu.nst; ++st, ++q) {
           if (seg_left == 0) {
             // a new accumulation segment: wait until its accumulator is free
             bi = p.promote ? 0 : (int)(u & 1);
@@ -302,9 +348,11 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           tc_fence_after();
           if (elect_one()) {
             const uint32_t dt = tmem + (uint32_t)bi * kAccCols;
-            const int t0 = st * p.T, t1 = min(g.R * g.S, t0 + p.T);
+            const int u0 = st * p.T, u1 = min(iu.nu, u0 + p.T);
             uint64_t sa = a_tmpl + stage0 + (uint32_t)s * stage16;
-            for (int tap = t0; tap < t1; ++tap, sa += chunk16) {
+            for (int u = u0; u < u1; ++u, sa += chunk16) {
+              // the tap whose operand the unit reads (paired: the first of two)
+              const int tap = (u / hs) * p.tstride + (PAIR ? 2 : 1) * (u % hs);
               const uint64_t hp = hdesc + (uint32_t)p.tap_phase[tap] * TERMS * part16 + (uint32_t)p.tap_off[tap];
               for (int j = 0; j < p.KS; ++j) {
 #pragma unroll
@@ -343,23 +391,23 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     // size, so each stage (T consecutive taps of one plane block, contiguous
     // in the packed operand) is one copy.
     if (lane == 0) {
-      const int RS = g.R * g.S;  // taps
       uint32_t q = 0;
       bool ok = true;
       for (int i = blockIdx.x; ok && i < p.total && !*abort_flag; i += gridDim.x) {
-        const Item it = decode(p, i);
-        const uint8_t *src = p.bpack + (size_t)it.nb * p.NCB * RS * p.chunk_bytes;
+        const ItemUnits iu = item_units<PAIR>(p, decode(p, i));
+        const int NU = iu.nu;
+        const uint8_t *src = p.bpack + iu.chunk0 * p.chunk_bytes;
         for (int cb = 0; ok && cb < p.NCB; ++cb)
-          for (int st = 0; st < p.nst; ++st, ++q) {
+          for (int st = 0; st < iu.nst; ++st, ++q) {
             const int s = q % p.stages;
             if (!mbar_wait(&bars.empty[s], ((q / p.stages) & 1) ^ 1, p.err)) {
               ok = false;
               break;
             }
             const int t0 = st * p.T;
-            const uint32_t bytes = (uint32_t)min(p.T, RS - t0) * p.chunk_bytes;
+            const uint32_t bytes = (uint32_t)min(p.T, NU - t0) * p.chunk_bytes;
             mbar_arrive_expect_tx(&bars.full[s], bytes);
-            bulk_load(stage + (size_t)s * p.stage_bytes, src + ((size_t)cb * RS + t0) * p.chunk_bytes, bytes,
+            bulk_load(stage + (size_t)s * p.stage_bytes, src + ((size_t)cb * NU + t0) * p.chunk_bytes, bytes,
                       &bars.full[s]);
           }
       }
@@ -372,29 +420,82 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     }
   } else {
     // ------------------------------------------------------------ epilogue
+    // Lane quarters: rows 0-63 hold hi*hi sums, rows 64-127 corrections; with
+    // paired taps rows 0-31 / 32-63 are tap a's (hi*hi, corrections) and rows
+    // 64-127 tap b's, one grid position to the right.  The warps holding one
+    // filter block's parts for the same columns combine through shared memory
+    // (a pair of warps, or with paired taps a group of four).
     const int ew = warp - kEpiWarp0;
     const int quarter = warp & 3;         // tensor-memory lanes this warp may access
     const int half = ew >> 2;             // column half
-    const bool big = quarter < 2;         // rows 0-63: hi*hi sums; 64-127: corrections
-    const int pair = (quarter & 1) * 2 + half;  // big warp + small warp of the same filters and columns
-    const int bar_id = 2 + pair;
+    const bool big = quarter < 2;
+    const int grp = PAIR ? half : (quarter & 1) * 2 + half;
+    const int bar_id = 2 + grp, bar_count = PAIR ? 128 : 64;
     const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
     const int ncol = p.N / 2, cbeg = half * ncol;
-    float *xp = xch + pair * 2 * kXchFloats;
+    float *xp = xch + grp * (PAIR ? 6 : 2) * kXchFloats;
     const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
     const size_t opl = (size_t)g.OH * g.OW;
+    const int limit = PAIR ? p.tile_adv : p.N;  // columns of the tile with complete sums
     uint32_t u = 0;
     bool failed = false;
     for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
       const Item it = decode(p, i);
-      const int p0 = it.tile * p.N;
-      const int bw = min(p.BW, g.OW - it.band * p.BW);  // valid columns of the band
-      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)it.band * p.BW;
+      const ItemUnits iu = item_units<PAIR>(p, it);
+      const int nseg = (p.NCB * iu.nst + p.seg_stages - 1) / p.seg_stages;  // accumulation segments
+      const int p0 = it.tile * p.tile_adv;
+      // grid position (Y, X) of band `band` -> output (up*Y + rho, up*(band*BW + X) + kap)
+      const int rho = it.ph / p.up, kap = it.ph - rho * p.up;
+      const int ohv = (g.OH - rho + p.up - 1) / p.up;                 // valid grid rows
+      const int bw = min(p.BW, (g.OW - kap + p.up - 1) / p.up - it.band * p.BW);  // valid columns of the band
+      const size_t ors = (size_t)p.up * g.OW;                          // output row stride of a grid row
+      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)rho * g.OW + (size_t)it.band * p.BW * p.up + kap;
+      // Stores the combined [32 filters][16 positions] of chunk column c from
+      // xt, two filters' positions (or 8 filters' float4s) per instruction.
+      auto store_chunk = [&](const float *xt, int c, int fb) {
+        float w[16];
+        if (p.vec4) {
+          // lane -> (filter 8i + lane/4, positions c + 4*(lane%4) .. +3):
+          // four outputs that are consecutive and 16-byte aligned
+          const int t = 4 * (lane & 3);
+          const int G = p0 + c + t;
+          const int Y = G / p.P, X = G - Y * p.P;
+          const bool ok = Y < ohv && X < bw && c + t < limit;
+          const int fbase = fb + (lane >> 2);
+          float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * ors + X;  // up == 1 here
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float *r = xt + (8 * i + (lane >> 2)) * kXchPitch + t;
+            w[4 * i] = r[0];
+            w[4 * i + 1] = r[1];
+            w[4 * i + 2] = r[2];
+            w[4 * i + 3] = r[3];
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (ok && fbase + 8 * i < g.groups)
+              *reinterpret_cast<float4 *>(yo + (size_t)(8 * i) * opl) =
+                  make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+        } else {
+          // lane -> (filter 2i + lane/16, position c + lane%16)
+          const int t = lane & 15;
+          const int G = p0 + c + t;
+          const int Y = G / p.P, X = G - Y * p.P;
+          const bool ok = Y < ohv && X < bw && c + t < limit;
+          const int fbase = fb + (lane >> 4);
+          float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * ors + (size_t)X * p.up;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) w[i] = xt[(2 * i + (lane >> 4)) * kXchPitch + t];
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (ok && fbase + 2 * i < g.groups) yo[(size_t)(2 * i) * opl] = w[i];
+        }
+      };
       for (int seg = 0; seg < nseg; ++seg, ++u) {
         const int bi = p.promote ? 0 : (int)(u & 1);
         const uint32_t use = p.promote ? u : (u >> 1);
         bool bad = *abort_flag != 0 || !mbar_wait(&bars.dfull[bi], use & 1, p.err);
-        bad = named_sync_or(bar_id, 64, bad);  // both warps of the pair agree
+        bad = named_sync_or(bar_id, bar_count, bad);  // the combining warps agree
         if (bad) {
           failed = true;
           break;
@@ -422,77 +523,78 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           if (lane == 0) mbar_arrive(&bars.dempty[bi]);
           continue;
         }
-        // last segment: out = S (+ R) for the big and the small rows of each
-        // filter, added in shared memory ([filter][16 positions] per chunk);
-        // then the big warp stores two filters' 16 positions per instruction
+        // last segment: out = S (+ R) for every part of each filter, added in
+        // shared memory ([filter][16 positions] per chunk), then stored
         int kb = 0;
         for (int c = cbeg; c < cbeg + ncol; c += 16, ++kb) {
-          uint32_t s16[16], r16[16];
+          uint32_t s16[16], r16[16], e1 = 0, e2 = 0;
           tmem_ld16(sc + c, s16);
           if (!first) tmem_ld16(rc + c, r16);
+          // paired taps: tap b's rows (quarters 2, 3) also need column c + 16
+          const bool ext = PAIR && quarter >= 2 && c + 16 < p.N;
+          if (ext) {
+            tmem_ld1(sc + c + 16, e1);
+            if (!first) tmem_ld1(rc + c + 16, e2);
+          }
           tc_wait_ld();
-          float v[16];
+          float v[17];
 #pragma unroll
           for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(s16[t]) + (first ? 0.0f : __uint_as_float(r16[t]));
+          v[16] = ext ? __uint_as_float(e1) + (first ? 0.0f : __uint_as_float(e2)) : 0.0f;
           if (c + 16 >= cbeg + ncol) {  // the accumulator is read: release it
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars.dempty[bi]);
           }
-          float *xt = xp + (kb & 1) * kXchFloats;  // [32 filters][pitch 17]
-          if (!big) {
+          if (PAIR) {
+            float *xt = xp + (kb & 1) * 3 * kXchFloats;  // parts: a's corrections, b's hi*hi, b's corrections
+            if (quarter != 0) {
+              float *part = xt + (quarter - 1) * kXchFloats;
+              const bool sh = quarter >= 2;  // tap b's sums sit one position to the right
 #pragma unroll
-            for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = v[t];
-          }
-          named_sync(bar_id, 64);
-          if (big) {
-            // every load of a batch is issued before the batch's stores
-            float w[16];
-#pragma unroll
-            for (int t = 0; t < 16; ++t) w[t] = xt[lane * kXchPitch + t];
-#pragma unroll
-            for (int t = 0; t < 16; ++t) {
-              w[t] += v[t];
-              if (relu) w[t] = fmaxf(w[t], 0.0f);
+              for (int t = 0; t < 16; ++t) part[lane * kXchPitch + t] = sh ? v[t + 1] : v[t];
             }
+            named_sync(bar_id, bar_count);
+            if (quarter == 0) {
+              float w[16], w1[16], w2[16];
 #pragma unroll
-            for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
-            __syncwarp();
-            if (p.vec4) {
-              // lane -> (filter 8i + lane/4, positions c + 4*(lane%4) .. +3):
-              // four outputs that are consecutive and 16-byte aligned
-              const int t = 4 * (lane & 3);
-              const int G = p0 + c + t;
-              const int Y = G / p.P, X = G - Y * p.P;
-              const bool ok = Y < g.OH && X < bw;
-              const int fbase = it.nb * 64 + (quarter & 1) * 32 + (lane >> 2);
-              float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * g.OW + X;
-#pragma unroll
-              for (int i = 0; i < 4; ++i) {
-                const float *r = xt + (8 * i + (lane >> 2)) * kXchPitch + t;
-                w[4 * i] = r[0];
-                w[4 * i + 1] = r[1];
-                w[4 * i + 2] = r[2];
-                w[4 * i + 3] = r[3];
+              for (int t = 0; t < 16; ++t) {
+                w[t] = xt[lane * kXchPitch + t];
+                w1[t] = xt[kXchFloats + lane * kXchPitch + t];
+                w2[t] = xt[2 * kXchFloats + lane * kXchPitch + t];
               }
 #pragma unroll
-              for (int i = 0; i < 4; ++i)
-                if (ok && fbase + 8 * i < g.groups)
-                  *reinterpret_cast<float4 *>(yo + (size_t)(8 * i) * opl) =
-                      make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
-            } else {
-              // lane -> (filter 2i + lane/16, position c + lane%16)
-              const int t = lane & 15;
-              const int G = p0 + c + t;
-              const int Y = G / p.P, X = G - Y * p.P;
-              const bool ok = Y < g.OH && X < bw;
-              const int fbase = it.nb * 64 + (quarter & 1) * 32 + (lane >> 4);
-              float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * g.OW + X;
+              for (int t = 0; t < 16; ++t) {
+                float val = ((v[t] + w[t]) + w1[t]) + w2[t];
+                if (relu) val = fmaxf(val, 0.0f);
+                w[t] = val;
+              }
 #pragma unroll
-              for (int i = 0; i < 16; ++i) w[i] = xt[(2 * i + (lane >> 4)) * kXchPitch + t];
+              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
+              __syncwarp();
+              store_chunk(xt, c, it.nb * p.fblock);
+            }
+          } else {
+            float *xt = xp + (kb & 1) * kXchFloats;  // [32 filters][pitch 17]
+            if (!big) {
 #pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if (ok && fbase + 2 * i < g.groups) yo[(size_t)(2 * i) * opl] = w[i];
+              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = v[t];
+            }
+            named_sync(bar_id, bar_count);
+            if (big) {
+              // every load of a batch is issued before the batch's stores
+              float w[16];
+#pragma unroll
+              for (int t = 0; t < 16; ++t) w[t] = xt[lane * kXchPitch + t];
+#pragma unroll
+              for (int t = 0; t < 16; ++t) {
+                w[t] += v[t];
+                if (relu) w[t] = fmaxf(w[t], 0.0f);
+              }
+#pragma unroll
+              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
+              __syncwarp();
+              store_chunk(xt, c, it.nb * p.fblock + (quarter & 1) * 32);
             }
           }
         }
@@ -508,16 +610,25 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
   if (warp == kMmaWarp) tmem_dealloc(tmem, 512);
 }
 
-// Pack the filter bank into per-chunk operand images: chunk (nb, cb, tap) =
-// arows x CB bf16, row blocks of 64 as block_term() lists, row n of a block =
-// filter nb*64 + n, column ci = plane cb*CB + ci, the filter value of the
-// tap (flipped for convolution).  Layout: core matrices of 8 rows x 8
-// columns (128 bytes), row groups SBO = CB*16 bytes apart, column groups
-// LBO = 128 bytes apart.  Rows or columns past the real counts are 0.
-__global__ void bank_pack_kernel(ConvGeom g, const float *__restrict__ f, uint8_t *__restrict__ out, int CB,
-                                 int NCB, int nblocks, int terms, int arows) {
-  const int RS = g.R * g.S;
-  const int total = nblocks * NCB * RS * arows * CB;
+// Pack the filter bank into per-chunk operand images: chunk (output phase,
+// nb, cb, unit) = arows x CB bf16, column ci = plane cb*CB + ci, the filter
+// value of the tap (flipped for convolution).  A unit is one tap, with row
+// blocks of 64 as block_term() lists and row n of a block = filter nb*64 + n;
+// or, paired, two taps a, a + 1 of a filter row, with row blocks of 32 as
+// pair_block_term() and pair_block_tap() list and row n of a block = filter
+// nb*32 + n (tap a + 1 past the row's end is 0).  With UpsampleInput the
+// taps of a unit are those of its phase's sub-filter.  Layout: core matrices
+// of 8 rows x 8 columns (128 bytes), row groups SBO = CB*16 bytes apart,
+// column groups LBO = 128 bytes apart.  Rows or columns past the real counts
+// are 0.
+template <bool PAIR>
+__global__ void bank_pack_kernel(const __grid_constant__ BankParams p, const float *__restrict__ f,
+                                 uint8_t *__restrict__ out) {
+  const ConvGeom &g = p.g;
+  const int CB = p.CB, arows = p.arows;
+  // every (phase, block, plane block, unit) slot of the largest phase; the
+  // units a phase lacks are skipped.  Below 2^31 (checked at launch).
+  const int total = p.nph_out * p.nblocks * p.NCB * p.nunits * arows * CB;
   // the previous kernel (the last launch that read the packed operand) must
   // be done before it is rewritten; the consuming kernel may be scheduled now
   grid_dependency_wait();
@@ -527,30 +638,54 @@ __global__ void bank_pack_kernel(ConvGeom g, const float *__restrict__ f, uint8_
     int rest = idx / CB;
     const int row = rest % arows;
     rest /= arows;
-    const int tap = rest % RS;
-    rest /= RS;
-    const int cb = rest % NCB;
-    const int nb = rest / NCB;
-    const int part = block_term(terms, row >> 6);
-    const int k = nb * 64 + (row & 63), c = cb * CB + ci;
+    const int unit = rest % p.nunits;
+    rest /= p.nunits;
+    const int cb = rest % p.NCB;
+    rest /= p.NCB;
+    const int nb = rest % p.nblocks;
+    Item it{};
+    it.ph = rest / p.nblocks;
+    it.nb = nb;
+    const ItemUnits iu = item_units<PAIR>(p, it);
+    if (unit >= iu.nu) continue;
+    const int hs = PAIR ? (iu.ts + 1) / 2 : iu.ts;
+    int part, k, ss;
+    if (PAIR) {
+      const int blk = row >> 5;
+      part = pair_block_term(blk);
+      k = nb * 32 + (row & 31);
+      ss = 2 * (unit % hs) + pair_block_tap(blk);
+    } else {
+      part = block_term(p.terms, row >> 6);
+      k = nb * 64 + (row & 63);
+      ss = unit % hs;
+    }
+    const int rr = unit / hs;
+    int r = rr, s = ss;
+    if (p.up > 1) {
+      const int rho = it.ph / p.up;
+      r = p.up_r0[rho] + p.up * rr;
+      s = p.up_s0[it.ph - rho * p.up] + p.up * ss;
+    }
+    const int c = cb * CB + ci;
     float v = 0.0f;
-    if (part >= 0 && k < g.groups && c < g.n) {
+    if (part >= 0 && ss < iu.ts && r < g.R && s < g.S && k < g.groups && c < g.n) {
       int ip, fp;
       plane_pair(g, k, c, &ip, &fp);  // output plane k of image 0, term c
-      const int r = tap / g.S, s = tap - r * g.S;
+      const int tap = r * g.S + s;
       const int src = g.orient == CCT_CONVOLUTION ? (g.R - 1 - r) * g.S + (g.S - 1 - s) : tap;
-      const float a = f[(size_t)fp * RS + src];
+      const float a = f[(size_t)fp * g.R * g.S + src];
       const float h = __bfloat162float(__float2bfloat16_rn(a));
       if (part == 0) {
         v = h;
-      } else if (terms == 2) {
+      } else if (p.terms == 2) {
         v = a - h;  // rounded to bf16 below
       } else {
         const float m = __bfloat162float(__float2bfloat16_rn(a - h));
         v = part == 1 ? m : (a - h) - m;
       }
     }
-    const size_t chunk = ((size_t)nb * NCB + cb) * RS + tap;
+    const size_t chunk = iu.chunk0 + (size_t)cb * iu.nu + unit;
     const uint32_t off = (uint32_t)((row >> 3) * (CB * 16) + (ci >> 3) * 128 + (row & 7) * 16 + (ci & 7) * 2);
     *reinterpret_cast<__nv_bfloat16 *>(out + chunk * ((size_t)arows * CB * 2) + off) = __float2bfloat16_rn(v);
   }
@@ -559,15 +694,15 @@ __global__ void bank_pack_kernel(ConvGeom g, const float *__restrict__ f, uint8_
 std::mutex g_bank_mu;
 std::unordered_map<uint64_t, size_t> g_bank_attr;
 
-template <int TERMS>
+template <int TERMS, bool PAIR>
 int launch_terms(const BankParams &p, cudaStream_t st) {
-  auto kern = bank_tc_kernel<TERMS>;
+  auto kern = bank_tc_kernel<TERMS, PAIR>;
   {
     // Dynamic shared memory above 48 KB needs the opt-in attribute; keep the
     // largest size set so far per (device, instance).
     int dev = 0;
     cudaGetDevice(&dev);
-    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)TERMS;
+    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)(TERMS * 2 + (PAIR ? 1 : 0));
     std::lock_guard<std::mutex> lk(g_bank_mu);
     size_t &have = g_bank_attr[key];
     if (have < p.smem_bytes) {
@@ -593,31 +728,86 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
   if (g.mode != CCT_PROJECT_FRAME_BLOCK_REDUCE_SUM && g.mode != CCT_BACK_PROJECT_FRAME_BLOCK_REDUCE_SUM)
     return false;
   if (terms != 2 && terms != 3) return false;
-  if (g.up != 1 || g.fup != 1 || g.down < 1 || g.down > 2) return false;
+  if (g.fup != 1 || g.down < 1 || g.down > 2 || g.up < 1 || g.up > kBankMaxUp) return false;
+  if (g.up > 1 && (g.down != 1 || g.border == CCT_BORDER_CLAMP)) return false;
   const int RS = g.R * g.S;
   if (RS > kBankMaxTaps || g.n < 1 || g.groups < 1) return false;
   BankParams p{};
   p.g = g;
   p.terms = terms;
-  p.nmma = terms == 2 ? 2 : 5;
-  p.arows = terms == 2 ? 192 : 448;
-  const int d = g.down;
-  // row / column shifts in strided units and the input phases the taps read
-  p.sr_min = floor_div(-g.low_r, d);
-  p.sc_min = floor_div(-g.low_c, d);
-  const int dr = floor_div(g.R - 1 - g.low_r, d) - p.sr_min;
-  const int dc = floor_div(g.S - 1 - g.low_c, d) - p.sc_min;
-  int phase_of[2][2] = {{-1, -1}, {-1, -1}};
-  for (int r = 0; r < g.R; ++r)
-    for (int s = 0; s < g.S; ++s) {
-      const int pr = pos_mod(r - g.low_r, d), pc = pos_mod(s - g.low_c, d);
-      if (phase_of[pr][pc] < 0) {
-        phase_of[pr][pc] = p.nphase;
-        p.phase_r[p.nphase] = pr;
-        p.phase_c[p.nphase] = pc;
-        ++p.nphase;
-      }
+  const int d = g.down, u = g.up;
+  p.up = u;
+  p.nph_out = u * u;
+  int dr, dc;  // reach of the (sub-)filter on the grid, rows and columns
+  int rq_max = 1, sq_max = 1;
+  if (u > 1) {
+    // UpsampleInput (ConvolveHyperKernel.scala:206-212, 405-459): output row
+    // i = u*I + rho takes filter rows r with (rho - low_r + r) % u == 0, that
+    // is r = r0 + u*rr, reading input row I + (rho - low_r + r0)/u + rr.
+    // Phases without such rows keep one zero sub-filter row, so every phase
+    // writes its outputs.
+    for (int ph = 0; ph < u; ++ph) {
+      const int r0 = pos_mod(g.low_r - ph, u), s0 = pos_mod(g.low_c - ph, u);
+      p.up_r0[ph] = r0;
+      p.up_s0[ph] = s0;
+      p.up_rq[ph] = std::max(1, r0 < g.R ? (g.R - 1 - r0) / u + 1 : 0);
+      p.up_sq[ph] = std::max(1, s0 < g.S ? (g.S - 1 - s0) / u + 1 : 0);
+      p.up_sr[ph] = floor_div(ph - g.low_r + r0, u);
+      p.up_sc[ph] = floor_div(ph - g.low_c + s0, u);
+      rq_max = std::max(rq_max, p.up_rq[ph]);
+      sq_max = std::max(sq_max, p.up_sq[ph]);
     }
+    dr = rq_max - 1;
+    dc = sq_max - 1;
+    p.OHq = (g.OH + u - 1) / u;
+    p.OWq = (g.OW + u - 1) / u;
+    p.nphase = 1;
+    p.tstride = sq_max;
+  } else {
+    // row / column shifts in strided units and the input phases the taps read
+    p.sr_min = floor_div(-g.low_r, d);
+    p.sc_min = floor_div(-g.low_c, d);
+    dr = floor_div(g.R - 1 - g.low_r, d) - p.sr_min;
+    dc = floor_div(g.S - 1 - g.low_c, d) - p.sc_min;
+    p.OHq = g.OH;
+    p.OWq = g.OW;
+    p.tstride = g.S;
+    rq_max = g.R;
+    sq_max = g.S;
+  }
+  if (rq_max * p.tstride > kBankMaxTaps) return false;
+  // Banks of at most 32 filters would leave half of each 128-row MMA empty:
+  // two taps of a filter row share it instead (stride-1 grids only, where
+  // tap a + 1 reads one grid position past tap a).
+  p.pair = (terms == 2 && g.groups <= 32 && d == 1 && sq_max >= 2) ? 1 : 0;
+  p.fblock = p.pair ? 32 : 64;
+  p.nblocks = (g.groups + p.fblock - 1) / p.fblock;
+  // units per phase: sub-filter rows x (columns, or column pairs)
+  auto units_of = [&](int rows, int cols) { return rows * (p.pair ? (cols + 1) / 2 : cols); };
+  p.nunits = 0;
+  for (int ph = 0; ph < p.nph_out; ++ph) {
+    const int nu = u > 1 ? units_of(p.up_rq[ph / u], p.up_sq[ph % u]) : units_of(g.R, g.S);
+    p.nunits = std::max(p.nunits, nu);
+  }
+  p.nmma = terms == 2 ? 2 : 5;
+  p.arows = p.pair ? 256 : terms == 2 ? 192 : 448;
+  const size_t xch_bytes = p.pair ? kXchBytesPair : kXchBytes;
+  const int NU = p.nunits;
+  int phase_of[2][2] = {{-1, -1}, {-1, -1}};
+  if (u > 1) {
+    phase_of[0][0] = 0;
+  } else {
+    for (int r = 0; r < g.R; ++r)
+      for (int s = 0; s < g.S; ++s) {
+        const int pr = pos_mod(r - g.low_r, d), pc = pos_mod(s - g.low_c, d);
+        if (phase_of[pr][pc] < 0) {
+          phase_of[pr][pc] = p.nphase;
+          p.phase_r[p.nphase] = pr;
+          p.phase_c[p.nphase] = pc;
+          ++p.nphase;
+        }
+      }
+  }
   // Band width BW, tile size N (positions) and plane block CB, by a cost
   // model: an M=128, 16-deep MMA over N positions takes N/2 tensor cycles and
   // reads 4 KB of filter plus 32*N bytes of halo from shared memory at about
@@ -634,14 +824,15 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
   bool found = false;
   double best_cost = 0.0;
   int best_cb = 0;
-  for (int bw : {g.OW, 512, 256, 192, 128, 96, 64, 48, 32}) {
-    if (bw > g.OW || (bw == g.OW && bw > 1024)) continue;
-    const int nbands = (g.OW + bw - 1) / bw;
-    const int BW = (g.OW + nbands - 1) / nbands;  // balanced bands
+  for (int bw : {p.OWq, 512, 256, 192, 128, 96, 64, 48, 32}) {
+    if (bw > p.OWq || (bw == p.OWq && bw > 1024)) continue;
+    const int nbands = (p.OWq + bw - 1) / bw;
+    const int BW = (p.OWq + nbands - 1) / nbands;  // balanced bands
     const int P = BW + dc;
-    const long long npos = (long long)g.OH * P;
+    const long long npos = (long long)p.OHq * P;
     for (int N : {256, 224, 192, 160, 128, 96, 64}) {
-      const long long tiles = (npos + N - 1) / N;
+      const int adv = p.pair ? N - 4 : N;  // paired: the last 4 positions of a tile lack tap b's sums
+      const long long tiles = (npos + adv - 1) / adv;
       const int L = ((N + dr * P + dc) + 7) & ~7;
       for (int CB : {64, 32, 16}) {
         if (CB > cmax && CB != 16) continue;
@@ -651,13 +842,13 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
         // taps per stage: about 1100 cycles of MMAs per bulk copy and per
         // stage hand-off, at least three stages
         const double tap_cycles = (CB / 16) * p.nmma * std::max(0.5 * N, 32.0 + 0.25 * N);
-        int T = std::min(RS, std::max(1, (int)std::ceil(1100.0 / tap_cycles)));
-        while (T > 1 && 2 * halo + 3 * T * chunk + kXchBytes > budget) --T;
-        if (2 * halo + 3 * T * chunk + kXchBytes > budget || L * 16 >= (1 << 18)) continue;
-        if (T * tap_cycles < 500.0 && T < RS && CB > 16) continue;  // a smaller plane block keeps stages long
+        int T = std::min(NU, std::max(1, (int)std::ceil(1100.0 / tap_cycles)));
+        while (T > 1 && 2 * halo + 3 * T * chunk + xch_bytes > budget) --T;
+        if (2 * halo + 3 * T * chunk + xch_bytes > budget || L * 16 >= (1 << 18)) continue;
+        if (T * tap_cycles < 500.0 && T < NU && CB > 16) continue;  // a smaller plane block keeps stages long
         // work items run in waves over the SMs: a small problem takes smaller
         // tiles to occupy more of them
-        const long long items = (long long)g.batch * nbands * tiles * ((g.groups + 63) / 64);
+        const long long items = (long long)g.batch * p.nph_out * nbands * tiles * p.nblocks;
         const double waves = (double)((items + sms - 1) / sms);
         const double cost = waves * (std::max(0.5 * N, 32.0 + 0.25 * N) + 8.0);
         if (!found || cost < best_cost * 0.999 || (cost <= best_cost * 1.001 && CB > best_cb)) {
@@ -672,7 +863,8 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
           p.chunk_bytes = (uint32_t)chunk;
           p.T = T;
           p.stage_bytes = (uint32_t)(T * chunk);
-          p.stages = (int)std::min<size_t>(6, (budget - 2 * halo - kXchBytes) / p.stage_bytes);
+          p.stages = (int)std::min<size_t>(6, (budget - 2 * halo - xch_bytes) / p.stage_bytes);
+          p.tile_adv = adv;
           p.tiles_band = (int)tiles;
           best_cost = cost;
           best_cb = CB;
@@ -683,41 +875,60 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
     }
   }
   if (!found) return false;
-  for (int tap = 0; tap < RS; ++tap) {
-    const int r = tap / g.S, s = tap % g.S;
-    const int ar = r - g.low_r, ac = s - g.low_c;
-    p.tap_phase[tap] = phase_of[pos_mod(ar, d)][pos_mod(ac, d)];
-    p.tap_off[tap] = (floor_div(ar, d) - p.sr_min) * p.P + (floor_div(ac, d) - p.sc_min);
+  if (u > 1) {
+    // sub-filter tap (rr, ss) of any phase: grid offset rr*P + ss
+    for (int rr = 0; rr < rq_max; ++rr)
+      for (int ss = 0; ss < sq_max; ++ss) {
+        p.tap_phase[rr * p.tstride + ss] = 0;
+        p.tap_off[rr * p.tstride + ss] = rr * p.P + ss;
+      }
+  } else {
+    for (int tap = 0; tap < RS; ++tap) {
+      const int r = tap / g.S, s = tap % g.S;
+      const int ar = r - g.low_r, ac = s - g.low_c;
+      p.tap_phase[tap] = phase_of[pos_mod(ar, d)][pos_mod(ac, d)];
+      p.tap_off[tap] = (floor_div(ar, d) - p.sr_min) * p.P + (floor_div(ac, d) - p.sc_min);
+    }
   }
-  p.nblocks = (g.groups + 63) / 64;
   p.NCB = (g.n + p.CB - 1) / p.CB;
   p.KS = p.CB / 16;
-  p.nst = (RS + p.T - 1) / p.T;
+  p.nst = (NU + p.T - 1) / p.T;
   const int tstages = p.NCB * p.nst;
   // Promotion: the hi*hi accumulator takes at most 64 k-steps (1024 terms of
   // the reduction) before it is added into the FP32 running sum.
   const int kmax = 64;
-  p.promote = p.NCB * RS * p.KS > kmax ? 1 : 0;
+  p.promote = p.NCB * NU * p.KS > kmax ? 1 : 0;
   p.seg_stages = p.promote ? std::max(1, kmax / (p.T * p.KS)) : tstages;
-  // float4 stores: groups of 4 grid positions (p0 and N are multiples of 4)
+  // float4 stores: groups of 4 grid positions (p0, N and tile_adv are multiples of 4)
   // never straddle a grid row or the band's last output column, and land on
   // 16-byte aligned outputs
-  p.vec4 = (p.P % 4 == 0 && p.BW % 4 == 0 && g.OW % 4 == 0 && p.N % 4 == 0) ? 1 : 0;
-  p.total = g.batch * p.nbands * p.tiles_band * p.nblocks;
-  if (p.total < 1) return false;
+  // (up-sampled outputs are strided: scalar stores)
+  p.vec4 = (u == 1 && p.P % 4 == 0 && p.BW % 4 == 0 && g.OW % 4 == 0 && p.N % 4 == 0) ? 1 : 0;
+  const long long total = (long long)g.batch * p.nph_out * p.nbands * p.tiles_band * p.nblocks;
+  if (total < 1 || total > 0x7fffffffLL) return false;
+  p.total = (int)total;
   p.grid = std::min(p.total, sms);
   p.smem_bytes = 2 * (size_t)p.halo_bytes + (size_t)p.stages * p.stage_bytes;
-  p.pack_bytes = (size_t)p.nblocks * p.NCB * RS * p.chunk_bytes;
+  // packed chunks: each output phase's filter blocks, plane blocks and units
+  size_t chunks = 0;
+  for (int ph = 0; ph < p.nph_out; ++ph) {
+    p.up_choff[ph] = (int)chunks;
+    const int nu = u > 1 ? units_of(p.up_rq[ph / u], p.up_sq[ph % u]) : NU;
+    chunks += (size_t)p.nblocks * p.NCB * nu;
+  }
+  p.pack_bytes = chunks * p.chunk_bytes;
   *out = p;
   return true;
 }
 
 int launch_bank_pack(const BankParams &p, const float *f, uint8_t *packed, cudaStream_t st) {
-  const long long total = (long long)p.nblocks * p.NCB * p.g.R * p.g.S * p.arows * p.CB;
+  const long long total = (long long)p.nph_out * p.nblocks * p.NCB * p.nunits * p.arows * p.CB;
   if (total > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "packed filter operand too large");
   const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-  const int rc = launch_pdl(bank_pack_kernel, dim3(blocks), dim3(256), 0, st, "bank_pack_kernel launch", p.g, f,
-                            packed, p.CB, p.NCB, p.nblocks, p.terms, p.arows);
+  const int rc = p.pair ? launch_pdl(bank_pack_kernel<true>, dim3(blocks), dim3(256), 0, st,
+                                     "bank_pack_kernel launch", p, f, packed)
+                        : launch_pdl(bank_pack_kernel<false>, dim3(blocks), dim3(256), 0, st,
+                                     "bank_pack_kernel launch", p, f, packed);
   if (rc) return rc;
   count_launches(1);
   return check_cuda(cudaGetLastError(), "bank_pack_kernel launch");
@@ -731,7 +942,8 @@ int launch_bank_tc(const BankParams &p, const float *x, float *y, const uint8_t 
   if ((reinterpret_cast<uintptr_t>(y) & 15) != 0) q.vec4 = 0;  // float4 stores need a 16-byte aligned output
   q.bpack = packed;
   q.err = err;
-  return p.terms == 2 ? launch_terms<2>(q, st) : launch_terms<3>(q, st);
+  if (p.pair) return launch_terms<2, true>(q, st);
+  return p.terms == 2 ? launch_terms<2, false>(q, st) : launch_terms<3, false>(q, st);
 }
 
 }  // namespace cct
@@ -740,15 +952,19 @@ namespace cct {
 
 bool frame_tc_choose(const ConvGeom &g, int precision, int sms, FrameTcChoice *out) {
   FrameTcChoice c{};
-  if (precision == CCT_PREC_BF16X3 && g.groups <= 32 && frame_tc_plan(g, sms, &c.tp)) {
-    c.bank = false;
-    c.pack_bytes = c.tp.pack_bytes;
-  } else if (bank_tc_plan(g, precision == CCT_PREC_BF16X6 ? 3 : 2, sms, &c.bp)) {
+  BankParams bp{};
+  const bool bank_ok = bank_tc_plan(g, precision == CCT_PREC_BF16X6 ? 3 : 2, sms, &bp);
+  if (bank_ok && (bp.pair || g.groups > 32 || precision != CCT_PREC_BF16X3)) {
     c.bank = true;
-    c.pack_bytes = c.bp.pack_bytes;
+    c.bp = bp;
+    c.pack_bytes = bp.pack_bytes;
   } else if (precision == CCT_PREC_BF16X3 && frame_tc_plan(g, sms, &c.tp)) {
     c.bank = false;
     c.pack_bytes = c.tp.pack_bytes;
+  } else if (bank_ok) {
+    c.bank = true;
+    c.bp = bp;
+    c.pack_bytes = bp.pack_bytes;
   } else {
     return false;
   }

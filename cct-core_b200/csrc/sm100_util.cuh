@@ -259,6 +259,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
       : "memory");
 }
 
+// 32 lanes x 1 column.
+__device__ __forceinline__ void tmem_ld1(uint32_t taddr, uint32_t &v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];\n" : "=r"(v) : "r"(taddr) : "memory");
+}
+
 // 1-D bulk copy global -> shared completing on `bar` (16-byte aligned, size % 16 == 0).
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(

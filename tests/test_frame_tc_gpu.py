@@ -100,6 +100,20 @@ TC_CASES = [
     (64, 520, 16, 16, 1, 5, O.CLAMP, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
     (40, 1027, 4, 16, 1, 9, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
     (64, 64, 32, 64, 2, 11, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    # banks of at most 32 filters: two taps per MMA (even, odd and 2-wide filters)
+    (40, 50, 3, 32, 2, 2, O.VALID, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (61, 67, 30, 40, 2, 6, O.FULL, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
+    (100, 1000, 24, 20, 1, 7, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (37, 29, 70, 31, 3, 9, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    # UpsampleInput: one sub-filter per output phase (ConvolveHyperKernel.scala:206-212, 405-459)
+    (32, 32, 32, 64, 2, 3, O.ZERO, O.UP, 2, O.BACKPROJECT_REDUCE),
+    (32, 32, 64, 32, 2, 3, O.ZERO, O.UP, 2, O.BACKPROJECT_REDUCE),
+    (32, 32, 32, 64, 2, 4, O.VALID, O.UP, 2, O.BACKPROJECT_REDUCE),
+    (17, 23, 70, 20, 2, 5, O.CYCLIC, O.UP, 2, O.PROJECT_REDUCE),
+    (20, 20, 8, 100, 2, 3, O.FULL, O.UP, 3, O.BACKPROJECT_REDUCE),
+    (16, 16, 8, 8, 1, 1, O.ZERO, O.UP, 2, O.PROJECT_REDUCE),
+    (30, 40, 16, 16, 2, 5, O.ZERO, O.UP, 4, O.BACKPROJECT_REDUCE),
+    (33, 31, 12, 40, 2, 6, O.FULL, O.UP, 2, O.PROJECT_REDUCE),
 ]
 
 
@@ -159,6 +173,7 @@ X6_CASES = [
     (64, 64, 32, 64, 2, 5, O.ZERO, O.NOSAMPLE, 1, O.BACKPROJECT_REDUCE),
     (40, 44, 17, 70, 2, 5, O.CYCLIC, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
     (48, 48, 3, 64, 2, 3, O.ZERO, O.NOSAMPLE, 1, O.PROJECT_REDUCE),
+    (40, 40, 64, 128, 2, 5, O.ZERO, O.UP, 2, O.BACKPROJECT_REDUCE),
 ]
 
 

@@ -221,6 +221,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
   // epilogue exchange: 4 warp pairs x 2 buffers, or (paired taps) 2 groups of
   // 4 warps x 3 parts x 2 buffers
   __shared__ float xch[(PAIR ? 12 : 8) * kXchFloats];
+  __shared__ uint32_t unit_boff[kBankMaxTaps];  // MMA warp: B operand offset of each unit
   const ConvGeom &g = p.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   uint8_t *halo = smem;                                 // 2 x halo_bytes
@@ -317,11 +318,38 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     const uint32_t chunk16 = p.chunk_bytes >> 4, part16 = p.part_bytes >> 4, stage16 = p.stage_bytes >> 4;
     const uint32_t kstep_b16 = 2u * p.L;              // B: two plane groups of L positions
     const uint32_t row16 = (uint32_t)p.CB / 8;        // A: one filter row (CB bf16) in 16-byte units
-    uint32_t q = 0, hb = 0, u = 0;
+    // The issuing thread's own latency bounds the stage rate, so the loop
+    // keeps to 32-bit descriptor words (the address field never carries into
+    // the stride fields), per-MMA operand offsets in registers, the B offset
+    // of each unit in a shared table, and stage / phase counters without
+    // divisions.
+    const uint32_t a_hi = (uint32_t)(a_tmpl >> 32), b_hi = (uint32_t)(b_tmpl >> 32);
+    const uint32_t a_lo0 = (uint32_t)a_tmpl + stage0, b_lo0 = (uint32_t)b_tmpl + halo0;
+    uint32_t aoff[ML::n], boff[ML::n];
+#pragma unroll
+    for (int m = 0; m < ML::n; ++m) {
+      aoff[m] = (uint32_t)ML::arow(m) * row16;
+      boff[m] = (uint32_t)ML::bterm(m) * part16;
+    }
+    int s = 0;             // stage slot
+    uint32_t sph = 0;      // parity of the slot's current fill
+    uint32_t hb = 0, u = 0;
+    int table_key = -1;    // (sub-filter width, units) the unit table holds
     bool failed = false;
     for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
       const ItemUnits iu = item_units<PAIR>(p, decode(p, i));
-      const int hs = PAIR ? (iu.ts + 1) / 2 : iu.ts;  // units per filter row
+      if (iu.ts * 1024 + iu.nu != table_key) {
+        // (re)written whenever the sub-filter width or the unit count changes
+        // (output phases of UpsampleInput), so every unit k < nu has its entry
+        // B offset of each unit (paired: of its first tap), in 16-byte units
+        const int hs = PAIR ? (iu.ts + 1) / 2 : iu.ts;  // units per filter row
+        for (int k = lane; k < iu.nu; k += 32) {
+          const int tap = (k / hs) * p.tstride + (PAIR ? 2 : 1) * (k % hs);
+          unit_boff[k] = (uint32_t)p.tap_phase[tap] * TERMS * part16 + (uint32_t)p.tap_off[tap];
+        }
+        __syncwarp();
+        table_key = iu.ts * 1024 + iu.nu;
+      }
       const int tstages = p.NCB * iu.nst;
       int seg_left = 0, done = 0, bi = 0;
       bool first = false;
@@ -330,8 +358,8 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         failed = __any_sync(0xffffffffu, *abort_flag || !mbar_wait(&bars.hfull[buf], (hb >> 1) & 1, p.err));
         if (failed) break;
         tc_fence_after();
-        const uint64_t hdesc = b_tmpl + halo0 + (uint32_t)buf * (p.halo_bytes >> 4);
-        for (int st = 0; st < iu.nst; ++st, ++q) {
+        const uint32_t hlo = b_lo0 + (uint32_t)buf * (p.halo_bytes >> 4);
+        for (int st = 0; st < iu.nst; ++st) {
           if (seg_left == 0) {
             // a new accumulation segment: wait until its accumulator is free
             bi = p.promote ? 0 : (int)(u & 1);
@@ -342,23 +370,20 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
             seg_left = min(p.seg_stages, tstages - done);
             first = true;
           }
-          const int s = q % p.stages;
-          failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[s], (q / p.stages) & 1, p.err));
+          failed = __any_sync(0xffffffffu, !mbar_wait(&bars.full[s], sph, p.err));
           if (failed) break;
           tc_fence_after();
           if (elect_one()) {
             const uint32_t dt = tmem + (uint32_t)bi * kAccCols;
             const int u0 = st * p.T, u1 = min(iu.nu, u0 + p.T);
-            uint64_t sa = a_tmpl + stage0 + (uint32_t)s * stage16;
-            for (int u = u0; u < u1; ++u, sa += chunk16) {
-              // the tap whose operand the unit reads (paired: the first of two)
-              const int tap = (u / hs) * p.tstride + (PAIR ? 2 : 1) * (u % hs);
-              const uint64_t hp = hdesc + (uint32_t)p.tap_phase[tap] * TERMS * part16 + (uint32_t)p.tap_off[tap];
+            uint32_t alo = a_lo0 + (uint32_t)s * stage16;
+            for (int k = u0; k < u1; ++k, alo += chunk16) {
+              const uint32_t blo = hlo + unit_boff[k];
               for (int j = 0; j < p.KS; ++j) {
 #pragma unroll
                 for (int m = 0; m < ML::n; ++m) {
-                  mma_bf16_ss(dt, sa + (uint32_t)ML::arow(m) * row16 + 16u * j,
-                              hp + (uint32_t)ML::bterm(m) * part16 + (uint32_t)j * kstep_b16, idesc,
+                  mma_bf16_ss(dt, desc_word(a_hi, alo + aoff[m] + 16u * j),
+                              desc_word(b_hi, blo + boff[m] + (uint32_t)j * kstep_b16), idesc,
                               (first && m == 0) ? 0u : 1u);
                   first = false;
                 }
@@ -367,6 +392,10 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
             tc_commit(&bars.empty[s]);  // the stage may be refilled once these MMAs are done
           }
           __syncwarp();
+          if (++s == p.stages) {
+            s = 0;
+            sph ^= 1u;
+          }
           first = false;
           ++done;
           if (--seg_left == 0) {
@@ -391,7 +420,9 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     // size, so each stage (T consecutive taps of one plane block, contiguous
     // in the packed operand) is one copy.
     if (lane == 0) {
-      uint32_t q = 0;
+      uint32_t q = 0;     // stages issued
+      int s = 0;          // stage slot
+      uint32_t sph = 0;   // parity of the slot's current fill
       bool ok = true;
       for (int i = blockIdx.x; ok && i < p.total && !*abort_flag; i += gridDim.x) {
         const ItemUnits iu = item_units<PAIR>(p, decode(p, i));
@@ -399,8 +430,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         const uint8_t *src = p.bpack + iu.chunk0 * p.chunk_bytes;
         for (int cb = 0; ok && cb < p.NCB; ++cb)
           for (int st = 0; st < iu.nst; ++st, ++q) {
-            const int s = q % p.stages;
-            if (!mbar_wait(&bars.empty[s], ((q / p.stages) & 1) ^ 1, p.err)) {
+            if (!mbar_wait(&bars.empty[s], sph ^ 1u, p.err)) {
               ok = false;
               break;
             }
@@ -409,6 +439,10 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
             mbar_arrive_expect_tx(&bars.full[s], bytes);
             bulk_load(stage + (size_t)s * p.stage_bytes, src + ((size_t)cb * NU + t0) * p.chunk_bytes, bytes,
                       &bars.full[s]);
+            if (++s == p.stages) {
+              s = 0;
+              sph ^= 1u;
+            }
           }
       }
       if (!ok) *abort_flag = 1;

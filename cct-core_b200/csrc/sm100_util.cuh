@@ -285,6 +285,12 @@ __device__ __forceinline__ uint64_t smem_desc_kmajor(uint32_t saddr, uint32_t lb
   return d;                // base offset 0, layout type 0 (no swizzle)
 }
 
+// A descriptor from its high word (strides, version) and low word (address,
+// leading byte offset).
+__device__ __forceinline__ uint64_t desc_word(uint32_t hi, uint32_t lo) {
+  return ((uint64_t)hi << 32) | lo;
+}
+
 // Instruction descriptor for kind::f16: bf16 A and B (K-major), f32 D.
 __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
   return (1u << 4)                      // D format f32

@@ -248,8 +248,12 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
   tc_fence_after();
   const uint32_t tmem = bars.tmem_slot;
   // Nothing above touches global memory, so it may overlap the previous
-  // kernel in the stream (programmatic serialisation).
-  grid_dependency_wait();
+  // kernel in the stream (programmatic serialisation).  When that kernel is
+  // this launch's own filter pack, only the packed operand is still being
+  // written: the pack waited for every earlier grid before it let this one
+  // start, so the input is complete and the output no longer read, and only
+  // the loader (which reads the packed operand) waits here.
+  if (!p.after_pack) grid_dependency_wait();
   allow_dependent_launch();
 
   volatile int *abort_flag = &bars.abort_flag;
@@ -420,6 +424,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     // size, so each stage (T consecutive taps of one plane block, contiguous
     // in the packed operand) is one copy.
     if (lane == 0) {
+      if (p.after_pack) grid_dependency_wait();
       uint32_t q = 0;     // stages issued
       int s = 0;          // stage slot
       uint32_t sph = 0;   // parity of the slot's current fill
@@ -969,8 +974,9 @@ int launch_bank_pack(const BankParams &p, const float *f, uint8_t *packed, cudaS
 }
 
 int launch_bank_tc(const BankParams &p, const float *x, float *y, const uint8_t *packed, unsigned *err,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool after_pack) {
   BankParams q = p;
+  q.after_pack = after_pack ? 1 : 0;
   q.x = x;
   q.y = y;
   if ((reinterpret_cast<uintptr_t>(y) & 15) != 0) q.vec4 = 0;  // float4 stores need a 16-byte aligned output
@@ -1011,8 +1017,8 @@ int frame_tc_pack(const FrameTcChoice &c, const float *f, uint8_t *packed, cudaS
 }
 
 int frame_tc_run(const FrameTcChoice &c, const float *x, float *y, const uint8_t *packed, unsigned *err,
-                 cudaStream_t st) {
-  if (c.bank) return launch_bank_tc(c.bp, x, y, packed, err, st);
+                 cudaStream_t st, bool after_pack) {
+  if (c.bank) return launch_bank_tc(c.bp, x, y, packed, err, st, after_pack);
   if ((reinterpret_cast<uintptr_t>(x) & 15) != 0)
     return set_error(CCT_EINVAL, "image pointer must be 16-byte aligned for the tensor-core path");
   return launch_frame_tc(c.tp, x, y, packed, err, st);

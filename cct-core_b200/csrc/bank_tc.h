@@ -61,6 +61,7 @@ struct BankParams {
   int grid;              // persistent CTAs
   size_t smem_bytes;     // dynamic shared memory
   size_t pack_bytes;     // bytes of the packed filter operand
+  int after_pack;        // 1: the preceding grid in the stream is this launch's filter pack
   const float *x;
   const uint8_t *bpack;
   float *y;
@@ -70,8 +71,9 @@ struct BankParams {
 // terms: 2 or 3.  False when the shape is outside what the kernel handles.
 bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out);
 int launch_bank_pack(const BankParams &p, const float *f, uint8_t *packed, cudaStream_t st);
+// after_pack: the launch directly follows its own filter pack on `st`.
 int launch_bank_tc(const BankParams &p, const float *x, float *y, const uint8_t *packed,
-                   unsigned *err, cudaStream_t st);
+                   unsigned *err, cudaStream_t st, bool after_pack = false);
 
 }  // namespace cct
 
@@ -94,7 +96,8 @@ struct FrameTcChoice {
 // precision: CCT_PREC_BF16X3 or CCT_PREC_BF16X6 (bank_tc only).
 bool frame_tc_choose(const ConvGeom &g, int precision, int sms, FrameTcChoice *out);
 int frame_tc_pack(const FrameTcChoice &c, const float *f, uint8_t *packed, cudaStream_t st);
+// after_pack: frame_tc_pack was the last launch on `st`.
 int frame_tc_run(const FrameTcChoice &c, const float *x, float *y, const uint8_t *packed, unsigned *err,
-                 cudaStream_t st);
+                 cudaStream_t st, bool after_pack = false);
 
 }  // namespace cct

@@ -538,9 +538,10 @@ int cct_conv_run(const cct_conv_plan *p, const float *x, const float *f, float *
   switch (p->algo) {
     case ALGO_FRAME_BF16X3: {
       int rc = CCT_OK;
-      if (f != p->static_filter || !p->packed_static) rc = frame_tc_pack(p->tc, f, p->packed, st);
+      const bool pack = f != p->static_filter || !p->packed_static;
+      if (pack) rc = frame_tc_pack(p->tc, f, p->packed, st);
       if (rc) return rc;
-      return frame_tc_run(p->tc, x, y, p->packed, p->err, st);
+      return frame_tc_run(p->tc, x, y, p->packed, p->err, st, pack);
     }
     case ALGO_FRAME_F32:
       return launch_frame_f32(p->g, x, f, y, st);

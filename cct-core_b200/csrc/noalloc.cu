@@ -101,5 +101,5 @@ extern "C" int cct_conv_run_noalloc(const cct_conv_desc *desc, const float *imag
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   rc = frame_tc_pack(tc, filter, scratch, st);
   if (rc) return rc;
-  return frame_tc_run(tc, image, out, scratch, status, st);
+  return frame_tc_run(tc, image, out, scratch, status, st, true);
 }

@@ -71,6 +71,17 @@ class ServeRequest(ctypes.Structure):
 SERVE_CONV, SERVE_GRAPH_STEP = 0, 1
 SERVE_PER_CALL = 0x1
 
+NODE_CONV, NODE_ADD, NODE_SUB, NODE_MUL, NODE_RELU, NODE_SCALE = range(6)
+
+
+class FieldShape(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_int32), ("cols", ctypes.c_int32), ("planes", ctypes.c_int32)]
+
+
+class CircuitNode(ctypes.Structure):
+    _fields_ = [("op", ctypes.c_int32), ("in0", ctypes.c_int32), ("in1", ctypes.c_int32),
+                ("scalar", ctypes.c_float), ("conv", ConvDesc)]
+
 # Every symbol include/cct_conv.h declares, with (restype, argtypes).
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -102,6 +113,18 @@ SIGNATURES = {
     "cct_graph_reset": (_I, [_P]),
     "cct_graph_save": (_I, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "cct_graph_restore": (_I, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "cct_circuit_assign": (_I, [ctypes.POINTER(FieldShape), _I32, ctypes.POINTER(CircuitNode), _I32, _PI32, _I32,
+                                _PI32, _PI32]),
+    "cct_circuit_create": (_I, [ctypes.POINTER(FieldShape), _I32, ctypes.POINTER(CircuitNode), _I32, _PI32, _I32,
+                                ctypes.POINTER(_P)]),
+    "cct_circuit_destroy": (_I, [_P]),
+    "cct_circuit_set_filter": (_I, [_P, _I32, _P]),
+    "cct_circuit_field": (_I, [_P, _I32, ctypes.POINTER(_P), ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_circuit_buffers": (_I, [_P, _PI32, ctypes.POINTER(ctypes.c_size_t)]),
+    "cct_circuit_step": (_I, [_P, ctypes.c_int64, _P]),
+    "cct_circuit_step_host": (_I, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
+    "cct_circuit_time": (ctypes.c_int64, [_P]),
+    "cct_circuit_reset": (_I, [_P]),
     "cct_conv_plan_save": (_I, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     "cct_conv_plan_restore": (_I, [_P, ctypes.c_size_t, ctypes.POINTER(_P)]),
     "cct_record_describe": (_I, [_P, ctypes.c_size_t, _PI32, _PI32, ctypes.POINTER(ctypes.c_int64),

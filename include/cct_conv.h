@@ -297,6 +297,74 @@ int cct_graph_save(const cct_graph *graph, uint32_t *words, size_t capacity,
                    size_t *n_words);
 int cct_graph_restore(const uint32_t *words, size_t n_words, cct_graph **graph);
 
+/* ---- kernel circuits (ComputeGraph step over a DAG) --------------------- */
+/* A ComputeGraph as a directed acyclic graph of operations over fields: the
+ * reference's KernelCircuit, enqueued in one fixed order every step
+ * (src/main/scala/cogx/runtime/execution/GPUSupervisor.scala:128-215), its
+ * fields packed into shared device buffers once nothing reads them any more
+ * (runtime/allocation/InOrderSharedLatchAllocator.scala:34: in-order
+ * execution, buffers binned by field size), inputs fed by sensors and
+ * results read by actuators (runtime/Sensor.scala:73).  The launches are
+ * captured once into a CUDA graph and every step replays it.
+ *
+ * Fields 0 .. n_inputs-1 are the inputs (sensors); field n_inputs + i is the
+ * output of node i.  Nodes are listed in execution order: a node reads only
+ * fields defined before it.  Inputs and the listed outputs keep buffers of
+ * their own; every other field shares a buffer of its size with fields whose
+ * last reader has run.
+ *
+ * cct_circuit_node   op CCT_NODE_CONV: `conv` describes the convolution, in0
+ *                    is its image field (shape as conv.image_*), in1 its
+ *                    filter field or -1 for a static filter set with
+ *                    cct_circuit_set_filter.  ADD / SUB / MUL: in0 op in1
+ *                    (equal element counts).  RELU: max(in0, 0).  SCALE:
+ *                    in0 * scalar.  Elementwise outputs take in0's shape.
+ * cct_circuit_assign the buffer assignment alone (host only, no device):
+ *                    field_buffer[n_inputs + n_nodes] and the buffer count.
+ * cct_circuit_create validates and plans every node, allocates the buffers
+ *                    (zeroed); CCT_EINVAL with a message naming the node.
+ * cct_circuit_step   `count` steps on `stream` (the first captures; fails
+ *                    with CCT_EINVAL while a static-filter node has none).
+ * cct_circuit_step_host  copies each host input in, steps once, copies each
+ *                    listed output to the host (synchronous).
+ * cct_circuit_buffers  device buffers in use and their bytes. */
+enum {
+  CCT_NODE_CONV = 0,
+  CCT_NODE_ADD = 1,
+  CCT_NODE_SUB = 2,
+  CCT_NODE_MUL = 3,
+  CCT_NODE_RELU = 4,
+  CCT_NODE_SCALE = 5
+};
+typedef struct {
+  int32_t rows, cols, planes; /* planes < 1: a scalar field (1 plane) */
+} cct_field_shape;
+typedef struct {
+  int32_t op;          /* CCT_NODE_*                                       */
+  int32_t in0, in1;    /* input fields; -1 where unused                    */
+  float scalar;        /* CCT_NODE_SCALE factor                            */
+  cct_conv_desc conv;  /* CCT_NODE_CONV                                    */
+} cct_circuit_node;
+typedef struct cct_circuit cct_circuit;
+int cct_circuit_assign(const cct_field_shape *inputs, int32_t n_inputs,
+                       const cct_circuit_node *nodes, int32_t n_nodes,
+                       const int32_t *outputs, int32_t n_outputs,
+                       int32_t *field_buffer, int32_t *n_buffers);
+int cct_circuit_create(const cct_field_shape *inputs, int32_t n_inputs,
+                       const cct_circuit_node *nodes, int32_t n_nodes,
+                       const int32_t *outputs, int32_t n_outputs,
+                       cct_circuit **out);
+int cct_circuit_destroy(cct_circuit *circuit);
+int cct_circuit_set_filter(cct_circuit *circuit, int32_t node, const float *host_filter);
+int cct_circuit_field(const cct_circuit *circuit, int32_t field, float **device_ptr,
+                      size_t *elems);
+int cct_circuit_buffers(const cct_circuit *circuit, int32_t *n_buffers, size_t *bytes);
+int cct_circuit_step(cct_circuit *circuit, int64_t count, void *stream);
+int cct_circuit_step_host(cct_circuit *circuit, const float *const *host_inputs,
+                          float *const *host_outputs, void *stream);
+int64_t cct_circuit_time(const cct_circuit *circuit);
+int cct_circuit_reset(cct_circuit *circuit);
+
 /* ---- request serving (continuous batching) ------------------------------ */
 /* No counterpart in the reference, whose ComputeGraphs are stepped by one
  * caller at a time.  A server serves one GPU with a scheduler thread.

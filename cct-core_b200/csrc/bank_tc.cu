@@ -45,9 +45,10 @@
 //   warp 9      loader (one lane): bulk copies of the pre-packed filter
 //               chunks (nb, plane block, tap) into a ring of stages.
 //   warps 10-17 epilogue, two per tensor-memory lane quarter (alternate
-//               column halves): promotion adds, then the big + small
-//               combination (small rows pass through shared memory to the
-//               warp holding the same filters' big rows), ReLU, stores.
+//               column halves): promotion adds, then per 16-column chunk the
+//               warps holding one filter block's parts write them to shared
+//               memory, and each adds the parts of a share of the filters,
+//               applies ReLU and stores.
 // Every wait is bounded: on a timeout the CTA records it in the device error
 // word, lets its copies and MMAs land, frees tensor memory and exits.
 #include <cuda_bf16.h>
@@ -72,12 +73,11 @@ constexpr int kEpiWarps = 8;
 constexpr int kThreads = 32 * (kEpiWarp0 + kEpiWarps);
 constexpr int kMaxStages = 8;
 constexpr uint32_t kAccCols = 256;  // one accumulator (N <= 256 fp32 columns)
-// Epilogue exchange: per warp pair two buffers of 32 filters x 16 positions
-// (row pitch 17 floats: conflict-free by filter and by position).
+// Epilogue exchange: eight part tiles of 32 filters x 16 positions (row
+// pitch 17 floats: conflict-free by filter and by position).
 constexpr int kXchPitch = 17;
 constexpr int kXchFloats = 32 * kXchPitch;
-constexpr size_t kXchBytes = 4 * 2 * kXchFloats * sizeof(float);
-constexpr size_t kXchBytesPair = 2 * 6 * kXchFloats * sizeof(float);
+constexpr size_t kXchBytes = 8 * kXchFloats * sizeof(float);
 
 // Filter chunk row blocks (64 rows each) and the MMAs over them.
 // Block contents: -1 zero, else the split term (0 hi, 1 mid / lo for 2 terms, 2 lo).
@@ -218,9 +218,8 @@ template <int TERMS, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_constant__ BankParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ Bars bars;
-  // epilogue exchange: 4 warp pairs x 2 buffers, or (paired taps) 2 groups of
-  // 4 warps x 3 parts x 2 buffers
-  __shared__ float xch[(PAIR ? 12 : 8) * kXchFloats];
+  // epilogue exchange: 4 groups of 2 part tiles, or (paired taps) 2 groups of 4
+  __shared__ float xch[8 * kXchFloats];
   __shared__ uint32_t unit_boff[kBankMaxTaps];  // MMA warp: B operand offset of each unit
   const ConvGeom &g = p.g;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -461,18 +460,22 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     // ------------------------------------------------------------ epilogue
     // Lane quarters: rows 0-63 hold hi*hi sums, rows 64-127 corrections; with
     // paired taps rows 0-31 / 32-63 are tap a's (hi*hi, corrections) and rows
-    // 64-127 tap b's, one grid position to the right.  The warps holding one
-    // filter block's parts for the same columns combine through shared memory
-    // (a pair of warps, or with paired taps a group of four).
+    // 64-127 tap b's, one grid position to the right.  The warps holding the
+    // parts of one block of 32 filters for the same columns form a group (two
+    // warps, or with paired taps four).  Per 16-column chunk each writes its
+    // part into its own [filter][position] tile, and after a barrier each adds
+    // the parts of its share of the filters (a half, or a quarter) and stores
+    // them, so no warp waits on another's stores.
+    constexpr int G = PAIR ? 4 : 2;  // parts (warps) per group
     const int ew = warp - kEpiWarp0;
     const int quarter = warp & 3;         // tensor-memory lanes this warp may access
     const int half = ew >> 2;             // column half
-    const bool big = quarter < 2;
     const int grp = PAIR ? half : (quarter & 1) * 2 + half;
-    const int bar_id = 2 + grp, bar_count = PAIR ? 128 : 64;
+    const int part = PAIR ? quarter : (quarter < 2 ? 0 : 1);  // this warp's part, and its share of filters
+    const int bar_id = 2 + grp, bar_count = 32 * G;
     const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
     const int ncol = p.N / 2, cbeg = half * ncol;
-    float *xp = xch + grp * (PAIR ? 6 : 2) * kXchFloats;
+    float *tiles = xch + grp * G * kXchFloats;  // the group's part tiles, [part][filter][pitch 17]
     const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
     const size_t opl = (size_t)g.OH * g.OW;
     const int limit = PAIR ? p.tile_adv : p.N;  // columns of the tile with complete sums
@@ -488,53 +491,15 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
       const int ohv = (g.OH - rho + p.up - 1) / p.up;                 // valid grid rows
       const int bw = min(p.BW, (g.OW - kap + p.up - 1) / p.up - it.band * p.BW);  // valid columns of the band
       const size_t ors = (size_t)p.up * g.OW;                          // output row stride of a grid row
-      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)rho * g.OW + (size_t)it.band * p.BW * p.up + kap;
-      // Stores the combined [32 filters][16 positions] of chunk column c from
-      // xt, two filters' positions (or 8 filters' float4s) per instruction.
-      auto store_chunk = [&](const float *xt, int c, int fb) {
-        float w[16];
-        if (p.vec4) {
-          // lane -> (filter 8i + lane/4, positions c + 4*(lane%4) .. +3):
-          // four outputs that are consecutive and 16-byte aligned
-          const int t = 4 * (lane & 3);
-          const int G = p0 + c + t;
-          const int Y = G / p.P, X = G - Y * p.P;
-          const bool ok = Y < ohv && X < bw && c + t < limit;
-          const int fbase = fb + (lane >> 2);
-          float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * ors + X;  // up == 1 here
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float *r = xt + (8 * i + (lane >> 2)) * kXchPitch + t;
-            w[4 * i] = r[0];
-            w[4 * i + 1] = r[1];
-            w[4 * i + 2] = r[2];
-            w[4 * i + 3] = r[3];
-          }
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (ok && fbase + 8 * i < g.groups)
-              *reinterpret_cast<float4 *>(yo + (size_t)(8 * i) * opl) =
-                  make_float4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
-        } else {
-          // lane -> (filter 2i + lane/16, position c + lane%16)
-          const int t = lane & 15;
-          const int G = p0 + c + t;
-          const int Y = G / p.P, X = G - Y * p.P;
-          const bool ok = Y < ohv && X < bw && c + t < limit;
-          const int fbase = fb + (lane >> 4);
-          float *yo = ybase0 + (size_t)fbase * opl + (size_t)Y * ors + (size_t)X * p.up;
-#pragma unroll
-          for (int i = 0; i < 16; ++i) w[i] = xt[(2 * i + (lane >> 4)) * kXchPitch + t];
-#pragma unroll
-          for (int i = 0; i < 16; ++i)
-            if (ok && fbase + 2 * i < g.groups) yo[(size_t)(2 * i) * opl] = w[i];
-        }
-      };
+      // the group's 32 filters
+      const int fb = it.nb * p.fblock + (PAIR ? 0 : (quarter & 1) * 32);
+      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)rho * g.OW + (size_t)it.band * p.BW * p.up + kap +
+                      (size_t)fb * opl;
       for (int seg = 0; seg < nseg; ++seg, ++u) {
         const int bi = p.promote ? 0 : (int)(u & 1);
         const uint32_t use = p.promote ? u : (u >> 1);
         bool bad = *abort_flag != 0 || !mbar_wait(&bars.dfull[bi], use & 1, p.err);
-        bad = named_sync_or(bar_id, bar_count, bad);  // the combining warps agree
+        bad = named_sync_or(bar_id, bar_count, bad);  // the group agrees
         if (bad) {
           failed = true;
           break;
@@ -562,20 +527,31 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           if (lane == 0) mbar_arrive(&bars.dempty[bi]);
           continue;
         }
-        // last segment: out = S (+ R) for every part of each filter, added in
-        // shared memory ([filter][16 positions] per chunk), then stored
-        int kb = 0;
-        for (int c = cbeg; c < cbeg + ncol; c += 16, ++kb) {
-          uint32_t s16[16], r16[16], e1 = 0, e2 = 0;
-          tmem_ld16(sc + c, s16);
-          if (!first) tmem_ld16(rc + c, r16);
+        // last segment: out = S (+ R) for every part of each filter.  The
+        // next chunk's accumulator load is in flight while a chunk is
+        // combined and stored (18 warps: 96 registers a thread at most).
+        uint32_t n16[16], ne = 0;
+        auto issue = [&](int c) {
+          tmem_ld16(sc + c, n16);
           // paired taps: tap b's rows (quarters 2, 3) also need column c + 16
-          const bool ext = PAIR && quarter >= 2 && c + 16 < p.N;
-          if (ext) {
-            tmem_ld1(sc + c + 16, e1);
-            if (!first) tmem_ld1(rc + c + 16, e2);
-          }
+          if (PAIR && quarter >= 2 && c + 16 < p.N) tmem_ld1(sc + c + 16, ne);
+        };
+        // (three-term and paired kernels load each chunk when they reach it:
+        // at 96 registers they have none for a load in flight)
+        constexpr bool kAhead = TERMS == 2 && !PAIR;
+        if (kAhead) issue(cbeg);
+        for (int c = cbeg; c < cbeg + ncol; c += 16) {
+          if (!kAhead) issue(c);
           tc_wait_ld();
+          const bool ext = PAIR && quarter >= 2 && c + 16 < p.N;
+          uint32_t s16[16], r16[16], e1 = ne, e2 = 0;
+#pragma unroll
+          for (int t = 0; t < 16; ++t) s16[t] = n16[t];
+          if (!first) {
+            tmem_ld16(rc + c, r16);
+            if (ext) tmem_ld1(rc + c + 16, e2);
+            tc_wait_ld();
+          }
           float v[17];
 #pragma unroll
           for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(s16[t]) + (first ? 0.0f : __uint_as_float(r16[t]));
@@ -585,55 +561,69 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars.dempty[bi]);
           }
-          if (PAIR) {
-            float *xt = xp + (kb & 1) * 3 * kXchFloats;  // parts: a's corrections, b's hi*hi, b's corrections
-            if (quarter != 0) {
-              float *part = xt + (quarter - 1) * kXchFloats;
-              const bool sh = quarter >= 2;  // tap b's sums sit one position to the right
+          {
+            float *mine = tiles + part * kXchFloats + lane * kXchPitch;
+            const bool sh = PAIR && quarter >= 2;  // tap b's sums sit one position to the right
 #pragma unroll
-              for (int t = 0; t < 16; ++t) part[lane * kXchPitch + t] = sh ? v[t + 1] : v[t];
-            }
-            named_sync(bar_id, bar_count);
-            if (quarter == 0) {
-              float w[16], w1[16], w2[16];
+            for (int t = 0; t < 16; ++t) mine[t] = sh ? v[t + 1] : v[t];
+          }
+          if (kAhead && c + 16 < cbeg + ncol) issue(c + 16);
+          named_sync(bar_id, bar_count);  // every part of the chunk is in place
+          // this warp's share: the parts of its filters, all loaded before the
+          // barrier that lets the group overwrite the tiles
+          float w[16];
+          int t0, fl;
+          if (p.vec4) {
+            // lane -> (filter 8*i + lane/4, positions 4*(lane%4) .. +3), i in the share
+            t0 = 4 * (lane & 3);
+            fl = lane >> 2;
 #pragma unroll
-              for (int t = 0; t < 16; ++t) {
-                w[t] = xt[lane * kXchPitch + t];
-                w1[t] = xt[kXchFloats + lane * kXchPitch + t];
-                w2[t] = xt[2 * kXchFloats + lane * kXchPitch + t];
+            for (int k = 0; k < 4 / G; ++k)
+#pragma unroll
+              for (int q = 0; q < G; ++q)
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                  w[(k * G + q) * 4 + e] = tiles[q * kXchFloats + (8 * (part * (4 / G) + k) + fl) * kXchPitch + t0 + e];
+          } else {
+            // lane -> (filter 2*i + lane/16, position lane%16), i in the share
+            t0 = lane & 15;
+            fl = lane >> 4;
+#pragma unroll
+            for (int k = 0; k < 16 / G; ++k)
+#pragma unroll
+              for (int q = 0; q < G; ++q)
+                w[k * G + q] = tiles[q * kXchFloats + (2 * (part * (16 / G) + k) + fl) * kXchPitch + t0];
+          }
+          named_sync(bar_id, bar_count);  // the tiles may be rewritten
+          const int Gp = p0 + c + t0;
+          const int Y = Gp / p.P, X = Gp - Y * p.P;
+          const bool ok = Y < ohv && X < bw && c + t0 < limit;
+          if (p.vec4) {
+            float *yo = ybase0 + (size_t)Y * ors + X;  // up == 1 here
+#pragma unroll
+            for (int k = 0; k < 4 / G; ++k) {
+              const int f = 8 * (part * (4 / G) + k) + fl;
+              float o[4];
+#pragma unroll
+              for (int e = 0; e < 4; ++e) {
+                float acc = w[(k * G) * 4 + e];
+#pragma unroll
+                for (int q = 1; q < G; ++q) acc = acc + w[(k * G + q) * 4 + e];  // parts in order
+                o[e] = relu ? fmaxf(acc, 0.0f) : acc;
               }
-#pragma unroll
-              for (int t = 0; t < 16; ++t) {
-                float val = ((v[t] + w[t]) + w1[t]) + w2[t];
-                if (relu) val = fmaxf(val, 0.0f);
-                w[t] = val;
-              }
-#pragma unroll
-              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
-              __syncwarp();
-              store_chunk(xt, c, it.nb * p.fblock);
+              if (ok && fb + f < g.groups)
+                *reinterpret_cast<float4 *>(yo + (size_t)f * opl) = make_float4(o[0], o[1], o[2], o[3]);
             }
           } else {
-            float *xt = xp + (kb & 1) * kXchFloats;  // [32 filters][pitch 17]
-            if (!big) {
+            float *yo = ybase0 + (size_t)Y * ors + (size_t)X * p.up;
 #pragma unroll
-              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = v[t];
-            }
-            named_sync(bar_id, bar_count);
-            if (big) {
-              // every load of a batch is issued before the batch's stores
-              float w[16];
+            for (int k = 0; k < 16 / G; ++k) {
+              const int f = 2 * (part * (16 / G) + k) + fl;
+              float acc = w[k * G];
 #pragma unroll
-              for (int t = 0; t < 16; ++t) w[t] = xt[lane * kXchPitch + t];
-#pragma unroll
-              for (int t = 0; t < 16; ++t) {
-                w[t] += v[t];
-                if (relu) w[t] = fmaxf(w[t], 0.0f);
-              }
-#pragma unroll
-              for (int t = 0; t < 16; ++t) xt[lane * kXchPitch + t] = w[t];
-              __syncwarp();
-              store_chunk(xt, c, it.nb * p.fblock + (quarter & 1) * 32);
+              for (int q = 1; q < G; ++q) acc = acc + w[k * G + q];  // parts in order
+              if (relu) acc = fmaxf(acc, 0.0f);
+              if (ok && fb + f < g.groups) yo[(size_t)f * opl] = acc;
             }
           }
         }
@@ -830,7 +820,7 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
   }
   p.nmma = terms == 2 ? 2 : 5;
   p.arows = p.pair ? 256 : terms == 2 ? 192 : 448;
-  const size_t xch_bytes = p.pair ? kXchBytesPair : kXchBytes;
+  const size_t xch_bytes = kXchBytes;
   const int NU = p.nunits;
   int phase_of[2][2] = {{-1, -1}, {-1, -1}};
   if (u > 1) {

@@ -59,6 +59,7 @@ struct BankParams {
   int promote;           // 1: segments are promoted into an FP32 running sum
   int vec4;              // 1: groups of 4 positions map to 4 aligned consecutive outputs (float4 stores)
   int grid;              // persistent CTAs
+  int sms;               // SMs of the device
   size_t smem_bytes;     // dynamic shared memory
   size_t pack_bytes;     // bytes of the packed filter operand
   int after_pack;        // 1: the preceding grid in the stream is this launch's filter pack

@@ -88,10 +88,11 @@ __host__ __device__ constexpr int block_term(int terms, int blk) {
                                                         : (blk == 1 ? 0 : blk == 2 ? 1 : blk == 4 ? 2 : 1));
 }
 // Paired taps (banks of at most 32 filters): a chunk of 32-row blocks
-// [Fh_a Fl_a Fh_b Fl_b 0 Fh_a 0 Fh_b] for taps a and b = a + 1 of one filter
-// row; -1 zero, else (term, which tap).
-__host__ __device__ constexpr int pair_block_term(int blk) { return blk == 4 || blk == 6 ? -1 : (blk & 1) && blk < 4 ? 1 : 0; }
-__host__ __device__ constexpr int pair_block_tap(int blk) { return blk == 2 || blk == 3 || blk == 7 ? 1 : 0; }
+// [0 0 Fh_a Fh_b Fl_a Fl_b] for taps a and b = a + 1 of one filter row, the
+// same 192 rows and MMAs as an unpaired two-term chunk: [Fh_a; Fh_b; Fl_a;
+// Fl_b] x Xh and [0; 0; Fh_a; Fh_b] x Xl.  -1 zero, else (term, which tap).
+__host__ __device__ constexpr int pair_block_term(int blk) { return blk < 2 ? -1 : blk < 4 ? 0 : 1; }
+__host__ __device__ constexpr int pair_block_tap(int blk) { return blk & 1; }
 template <int TERMS, bool PAIR>
 struct MmaList;
 template <>
@@ -101,12 +102,7 @@ struct MmaList<2, false> {
   __device__ static int bterm(int m) { return m; }               // Xh, Xl
 };
 template <>
-struct MmaList<2, true> {
-  static constexpr int n = 2;
-  // [Fh_a; Fl_a; Fh_b; Fl_b] x Xh, [0; Fh_a; 0; Fh_b] x Xl, at tap a's offset
-  __device__ static int arow(int m) { return m == 0 ? 0 : 128; }
-  __device__ static int bterm(int m) { return m; }
-};
+struct MmaList<2, true> : MmaList<2, false> {};  // at tap a's offset
 template <>
 struct MmaList<3, false> {
   static constexpr int n = 5;
@@ -460,8 +456,8 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
   } else {
     // ------------------------------------------------------------ epilogue
     // Lane quarters: rows 0-63 hold hi*hi sums, rows 64-127 corrections; with
-    // paired taps rows 0-31 / 32-63 are tap a's (hi*hi, corrections) and rows
-    // 64-127 tap b's, one grid position to the right.  The warps holding the
+    // paired taps the quarters are tap a's hi*hi, tap b's hi*hi, a's and b's
+    // corrections, tap b's one grid position to the right.  The warps holding the
     // parts of one block of 32 filters for the same columns form a group (two
     // warps, or with paired taps four).  Per 16-column chunk each writes its
     // part into its own [filter][position] tile, and after a barrier each adds
@@ -534,8 +530,8 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         uint32_t n16[16], ne = 0;
         auto issue = [&](int c) {
           tmem_ld16(sc + c, n16);
-          // paired taps: tap b's rows (quarters 2, 3) also need column c + 16
-          if (PAIR && quarter >= 2 && c + 16 < p.N) tmem_ld1(sc + c + 16, ne);
+          // paired taps: tap b's rows (quarters 1, 3) also need column c + 16
+          if (PAIR && (quarter & 1) && c + 16 < p.N) tmem_ld1(sc + c + 16, ne);
         };
         // (three-term and paired kernels load each chunk when they reach it:
         // at 96 registers they have none for a load in flight)
@@ -544,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         for (int c = cbeg; c < cbeg + ncol; c += 16) {
           if (!kAhead) issue(c);
           tc_wait_ld();
-          const bool ext = PAIR && quarter >= 2 && c + 16 < p.N;
+          const bool ext = PAIR && (quarter & 1) && c + 16 < p.N;
           uint32_t s16[16], r16[16], e1 = ne, e2 = 0;
 #pragma unroll
           for (int t = 0; t < 16; ++t) s16[t] = n16[t];
@@ -564,7 +560,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           }
           {
             float *mine = tiles + part * kXchFloats + lane * kXchPitch;
-            const bool sh = PAIR && quarter >= 2;  // tap b's sums sit one position to the right
+            const bool sh = PAIR && (quarter & 1);  // tap b's sums sit one position to the right
 #pragma unroll
             for (int t = 0; t < 16; ++t) mine[t] = sh ? v[t + 1] : v[t];
           }
@@ -843,7 +839,7 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
     p.nunits = std::max(p.nunits, nu);
   }
   p.nmma = terms == 2 ? 2 : 5;
-  p.arows = p.pair ? 256 : terms == 2 ? 192 : 448;
+  p.arows = terms == 2 ? 192 : 448;
   const size_t xch_bytes = kXchBytes;
   const int NU = p.nunits;
   int phase_of[2][2] = {{-1, -1}, {-1, -1}};

@@ -888,12 +888,19 @@ bool bank_tc_plan(const ConvGeom &g, int terms, int sms, BankParams *out) {
         const size_t part = (size_t)L * CB * 2;
         const size_t halo = (((size_t)p.nphase * terms * part) + 127) & ~(size_t)127;
         const size_t chunk = (size_t)p.arows * CB * 2;
-        // taps per stage: about 1100 cycles of MMAs per bulk copy and per
-        // stage hand-off, at least three stages
+        // Units per stage: each stage hand-off (the MMA thread's wait and
+        // commit, the loader's refill) costs ~400 cycles of the issuing
+        // thread's latency whatever the stage holds, so a stage takes as many
+        // units as fit, up to ~2000 cycles of MMAs, in three stages; two
+        // stages do when a stage holds at least ~1500 cycles of MMAs, enough
+        // to cover the refill of the other (measured: 12 MMAs of N = 256 in
+        // two stages beat 8 in three).
         const double tap_cycles = (CB / 16) * p.nmma * std::max(0.5 * N, 32.0 + 0.25 * N);
-        int T = std::min(NU, std::max(1, (int)std::ceil(1100.0 / tap_cycles)));
-        while (T > 1 && 2 * halo + 3 * T * chunk + xch_bytes > budget) --T;
-        if (2 * halo + 3 * T * chunk + xch_bytes > budget || L * 16 >= (1 << 18)) continue;
+        auto fits = [&](int t, int st) { return 2 * halo + (size_t)st * t * chunk + xch_bytes <= budget; };
+        auto ok_stages = [&](int t) { return fits(t, 3) || (fits(t, 2) && t * tap_cycles >= 1500.0); };
+        int T = std::min(NU, std::max(1, (int)(2000.0 / tap_cycles)));
+        while (T > 1 && !ok_stages(T)) --T;
+        if (!ok_stages(T) || L * 16 >= (1 << 18)) continue;
         if (T * tap_cycles < 500.0 && T < NU && CB > 16) continue;  // a smaller plane block keeps stages long
         // work items run in waves over the SMs: a small problem takes smaller
         // tiles to occupy more of them

@@ -211,6 +211,141 @@ __device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, 
   }
 }
 
+// Final accumulator of work item `it` (S in tensor-memory columns at `sc`,
+// plus the running sum at `rc` unless `first`), columns [cbeg, cbeg + ncol):
+// the group of G warps holding one block of 32 filters' parts (this warp's
+// lane quarter `quarter`, part `part`) writes each 16-column chunk into its
+// own [filter][position] tile, and after a barrier each adds the parts of its
+// share of the filters (a half, or a quarter) and stores them, so no warp
+// waits on another's stores.  `release` (or null): arrived on once this
+// warp's last accumulator load is done.
+template <int TERMS, bool PAIR>
+__device__ __forceinline__ void store_tile_columns(const BankParams &p, const Item &it, uint32_t sc, uint32_t rc,
+                                                   bool first, int cbeg, int ncol, float *tiles, int bar_id,
+                                                   int quarter, int part, int lane, uint64_t *release) {
+  const ConvGeom &g = p.g;
+  constexpr int G = PAIR ? 4 : 2;  // parts (warps) per group
+  const int bar_count = 32 * G;
+  const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
+  const size_t opl = (size_t)g.OH * g.OW;
+  const int limit = PAIR ? p.tile_adv : p.N;  // columns of the tile with complete sums
+  const int p0 = it.tile * p.tile_adv;
+  // grid position (Y, X) of band `band` -> output (up*Y + rho, up*(band*BW + X) + kap)
+  const int rho = it.ph / p.up, kap = it.ph - rho * p.up;
+  const int ohv = (g.OH - rho + p.up - 1) / p.up;                                 // valid grid rows
+  const int bw = min(p.BW, (g.OW - kap + p.up - 1) / p.up - it.band * p.BW);     // valid columns of the band
+  const size_t ors = (size_t)p.up * g.OW;                                          // output row stride of a grid row
+  // the group's 32 filters
+  const int fb = it.nb * p.fblock + (PAIR ? 0 : (quarter & 1) * 32);
+  float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)rho * g.OW + (size_t)it.band * p.BW * p.up + kap +
+                  (size_t)fb * opl;
+  // The next chunk's accumulator load is in flight while a chunk is combined
+  // and stored (18 warps: 96 registers a thread at most; three-term and
+  // paired kernels have none to spare and load each chunk when they reach it).
+  uint32_t n16[16], ne = 0;
+  auto issue = [&](int c) {
+    tmem_ld16(sc + c, n16);
+    // paired taps: tap b's rows (quarters 1, 3) also need column c + 16
+    if (PAIR && (quarter & 1) && c + 16 < p.N) tmem_ld1(sc + c + 16, ne);
+  };
+  constexpr bool kAhead = TERMS == 2 && !PAIR;
+  if (kAhead) issue(cbeg);
+  for (int c = cbeg; c < cbeg + ncol; c += 16) {
+    if (!kAhead) issue(c);
+    tc_wait_ld();
+    const bool ext = PAIR && (quarter & 1) && c + 16 < p.N;
+    uint32_t s16[16], r16[16], e1 = ne, e2 = 0;
+#pragma unroll
+    for (int t = 0; t < 16; ++t) s16[t] = n16[t];
+    if (!first) {
+      tmem_ld16(rc + c, r16);
+      if (ext) tmem_ld1(rc + c + 16, e2);
+      tc_wait_ld();
+    }
+    float v[17];
+#pragma unroll
+    for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(s16[t]) + (first ? 0.0f : __uint_as_float(r16[t]));
+    v[16] = ext ? __uint_as_float(e1) + (first ? 0.0f : __uint_as_float(e2)) : 0.0f;
+    if (release && c + 16 >= cbeg + ncol) {  // the accumulator is read: release it
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(release);
+    }
+    {
+      float *mine = tiles + part * kXchFloats + lane * kXchPitch;
+      const bool sh = PAIR && (quarter & 1);  // tap b's sums sit one position to the right
+#pragma unroll
+      for (int t = 0; t < 16; ++t) mine[t] = sh ? v[t + 1] : v[t];
+    }
+    if (kAhead && c + 16 < cbeg + ncol) issue(c + 16);
+    named_sync(bar_id, bar_count);  // every part of the chunk is in place
+    // this warp's share: the parts of its filters, all loaded before the
+    // barrier that lets the group overwrite the tiles
+    float w[16];
+    int t0, fl;
+    if (p.vec4) {
+      // lane -> (filter 8*i + lane/4, positions 4*(lane%4) .. +3), i in the share
+      t0 = 4 * (lane & 3);
+      fl = lane >> 2;
+#pragma unroll
+      for (int k = 0; k < 4 / G; ++k)
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+#pragma unroll
+          for (int e = 0; e < 4; ++e)
+            w[(k * G + q) * 4 + e] = tiles[q * kXchFloats + (8 * (part * (4 / G) + k) + fl) * kXchPitch + t0 + e];
+    } else {
+      // lane -> (filter 2*i + lane/16, position lane%16), i in the share
+      t0 = lane & 15;
+      fl = lane >> 4;
+#pragma unroll
+      for (int k = 0; k < 16 / G; ++k)
+#pragma unroll
+        for (int q = 0; q < G; ++q)
+          w[k * G + q] = tiles[q * kXchFloats + (2 * (part * (16 / G) + k) + fl) * kXchPitch + t0];
+    }
+    named_sync(bar_id, bar_count);  // the tiles may be rewritten
+    const int Gp = p0 + c + t0;
+    const int Y = Gp / p.P, X = Gp - Y * p.P;
+    const bool ok = Y < ohv && X < bw && c + t0 < limit;
+    if (p.vec4) {
+      float *yo = ybase0 + (size_t)Y * ors + X;  // up == 1 here
+#pragma unroll
+      for (int k = 0; k < 4 / G; ++k) {
+        const int f = 8 * (part * (4 / G) + k) + fl;
+        float o[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          float acc = w[(k * G) * 4 + e];
+#pragma unroll
+          for (int q = 1; q < G; ++q) acc = acc + w[(k * G + q) * 4 + e];  // parts in order
+          o[e] = relu ? fmaxf(acc, 0.0f) : acc;
+        }
+        if (ok && fb + f < g.groups)
+          *reinterpret_cast<float4 *>(yo + (size_t)f * opl) = make_float4(o[0], o[1], o[2], o[3]);
+      }
+    } else {
+      float *yo = ybase0 + (size_t)Y * ors + (size_t)X * p.up;
+#pragma unroll
+      for (int k = 0; k < 16 / G; ++k) {
+        const int f = 2 * (part * (16 / G) + k) + fl;
+        float acc = w[k * G];
+#pragma unroll
+        for (int q = 1; q < G; ++q) acc = acc + w[k * G + q];  // parts in order
+        if (relu) acc = fmaxf(acc, 0.0f);
+        if (ok && fb + f < g.groups) yo[(size_t)f * opl] = acc;
+      }
+    }
+  }
+}
+
+// The last tile of a CTA is stored by the converter warps as well as the
+// epilogue warps (each taking a quarter of the columns): by then the
+// converters have nothing left to fill.  Only when every item is one
+// accumulation segment (the converters then wait on the last item's
+// accumulator phase in order) and a quarter of a tile is whole chunks.
+__device__ __forceinline__ bool helpers_store_last(const BankParams &p) { return !p.promote && p.N % 64 == 0; }
+
 template <int TERMS, bool PAIR>
 __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_constant__ BankParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -305,6 +440,38 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
       }
     }
     if (failed) *abort_flag = 1;
+    if (helpers_store_last(p) && blockIdx.x < p.total) {
+      // The CTA's last tile, upper half of the columns: wait for its
+      // accumulator (one segment per item, so the phases of each buffer are
+      // waited in order), then store through tiles in the halo, which no MMA
+      // reads any more.
+      constexpr int G = PAIR ? 4 : 2;
+      int i_last = blockIdx.x, nitems = 0;
+      for (int i = blockIdx.x; i < p.total; i += gridDim.x, ++nitems) i_last = i;
+      const uint32_t u = (uint32_t)nitems - 1;  // the last item's segment (one per item)
+      const int bi = (int)(u & 1);
+      const uint32_t use = u >> 1;
+      const int quarter = warp & 3, chalf = warp >> 2;  // converter warps 0-7: lane quarter, column quarter
+      const int grp = PAIR ? chalf : (quarter & 1) * 2 + chalf;
+      const int part = PAIR ? quarter : (quarter < 2 ? 0 : 1);
+      const int bar_id = 6 + grp;  // epilogue groups use 2-5
+      // every converter warp comes here, failed or not, so both (or all
+      // four) warps of a group reach the barrier; they agree to skip if any
+      // of them failed or the wait gives up
+      bool bad = failed || *abort_flag != 0;
+      if (!bad) bad = !mbar_wait(&bars.dfull[bi], use & 1, p.err);
+      bad = named_sync_or(bar_id, 32 * G, bad);
+      if (!bad) {
+        tc_fence_after();
+        const uint32_t sc = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)bi * kAccCols;
+        float *tiles = reinterpret_cast<float *>(halo) + grp * G * kXchFloats;
+        const int ncol = p.N / 4;
+        store_tile_columns<TERMS, PAIR>(p, decode(p, i_last), sc, sc, true, p.N / 2 + chalf * ncol, ncol, tiles,
+                                        bar_id, quarter, part, lane, nullptr);
+      } else {
+        *abort_flag = 1;
+      }
+    }
   } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
     using ML = MmaList<TERMS, PAIR>;
@@ -457,12 +624,9 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     // ------------------------------------------------------------ epilogue
     // Lane quarters: rows 0-63 hold hi*hi sums, rows 64-127 corrections; with
     // paired taps the quarters are tap a's hi*hi, tap b's hi*hi, a's and b's
-    // corrections, tap b's one grid position to the right.  The warps holding the
-    // parts of one block of 32 filters for the same columns form a group (two
-    // warps, or with paired taps four).  Per 16-column chunk each writes its
-    // part into its own [filter][position] tile, and after a barrier each adds
-    // the parts of its share of the filters (a half, or a quarter) and stores
-    // them, so no warp waits on another's stores.
+    // corrections, tap b's one grid position to the right.  The warps holding
+    // the parts of one block of 32 filters for the same columns form a group
+    // (two warps, or with paired taps four): store_tile_columns.
     constexpr int G = PAIR ? 4 : 2;  // parts (warps) per group
     const int ew = warp - kEpiWarp0;
     const int quarter = warp & 3;         // tensor-memory lanes this warp may access
@@ -471,27 +635,18 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
     const int part = PAIR ? quarter : (quarter < 2 ? 0 : 1);  // this warp's part, and its share of filters
     const int bar_id = 2 + grp, bar_count = 32 * G;
     const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-    const int ncol = p.N / 2, cbeg = half * ncol;
     float *tiles = xch + grp * G * kXchFloats;  // the group's part tiles, [part][filter][pitch 17]
-    const bool relu = (g.flags & CCT_FLAG_RELU) != 0;
-    const size_t opl = (size_t)g.OH * g.OW;
-    const int limit = PAIR ? p.tile_adv : p.N;  // columns of the tile with complete sums
+    const bool helped = helpers_store_last(p);
     uint32_t u = 0;
     bool failed = false;
     for (int i = blockIdx.x; i < p.total && !failed; i += gridDim.x) {
       const Item it = decode(p, i);
       const ItemUnits iu = item_units<PAIR>(p, it);
       const int nseg = (p.NCB * iu.nst + p.seg_stages - 1) / p.seg_stages;  // accumulation segments
-      const int p0 = it.tile * p.tile_adv;
-      // grid position (Y, X) of band `band` -> output (up*Y + rho, up*(band*BW + X) + kap)
-      const int rho = it.ph / p.up, kap = it.ph - rho * p.up;
-      const int ohv = (g.OH - rho + p.up - 1) / p.up;                 // valid grid rows
-      const int bw = min(p.BW, (g.OW - kap + p.up - 1) / p.up - it.band * p.BW);  // valid columns of the band
-      const size_t ors = (size_t)p.up * g.OW;                          // output row stride of a grid row
-      // the group's 32 filters
-      const int fb = it.nb * p.fblock + (PAIR ? 0 : (quarter & 1) * 32);
-      float *ybase0 = p.y + (size_t)it.b * g.groups * opl + (size_t)rho * g.OW + (size_t)it.band * p.BW * p.up + kap +
-                      (size_t)fb * opl;
+      // the CTA's last tile: the converters store the upper half of the columns
+      const bool last_item = i + (int)gridDim.x >= p.total;
+      const int ncol = (helped && last_item) ? p.N / 4 : p.N / 2;
+      const int cbeg = half * ncol;
       for (int seg = 0; seg < nseg; ++seg, ++u) {
         const int bi = p.promote ? 0 : (int)(u & 1);
         const uint32_t use = p.promote ? u : (u >> 1);
@@ -506,8 +661,8 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         const uint32_t rc = tmem + lane_base + kAccCols;  // running sum (promotion)
         const bool first = seg == 0, last = seg == nseg - 1;
         if (!last) {
-          // promotion: R (+)= S, FP32 round to nearest
-          for (int c = cbeg; c < cbeg + ncol; c += 16) {
+          // promotion: R (+)= S, FP32 round to nearest, over the warp's column half
+          for (int c = half * (p.N / 2); c < (half + 1) * (p.N / 2); c += 16) {
             uint32_t s16[16], r16[16];
             tmem_ld16(sc + c, s16);
             if (!first) tmem_ld16(rc + c, r16);
@@ -524,106 +679,9 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
           if (lane == 0) mbar_arrive(&bars.dempty[bi]);
           continue;
         }
-        // last segment: out = S (+ R) for every part of each filter.  The
-        // next chunk's accumulator load is in flight while a chunk is
-        // combined and stored (18 warps: 96 registers a thread at most).
-        uint32_t n16[16], ne = 0;
-        auto issue = [&](int c) {
-          tmem_ld16(sc + c, n16);
-          // paired taps: tap b's rows (quarters 1, 3) also need column c + 16
-          if (PAIR && (quarter & 1) && c + 16 < p.N) tmem_ld1(sc + c + 16, ne);
-        };
-        // (three-term and paired kernels load each chunk when they reach it:
-        // at 96 registers they have none for a load in flight)
-        constexpr bool kAhead = TERMS == 2 && !PAIR;
-        if (kAhead) issue(cbeg);
-        for (int c = cbeg; c < cbeg + ncol; c += 16) {
-          if (!kAhead) issue(c);
-          tc_wait_ld();
-          const bool ext = PAIR && (quarter & 1) && c + 16 < p.N;
-          uint32_t s16[16], r16[16], e1 = ne, e2 = 0;
-#pragma unroll
-          for (int t = 0; t < 16; ++t) s16[t] = n16[t];
-          if (!first) {
-            tmem_ld16(rc + c, r16);
-            if (ext) tmem_ld1(rc + c + 16, e2);
-            tc_wait_ld();
-          }
-          float v[17];
-#pragma unroll
-          for (int t = 0; t < 16; ++t) v[t] = __uint_as_float(s16[t]) + (first ? 0.0f : __uint_as_float(r16[t]));
-          v[16] = ext ? __uint_as_float(e1) + (first ? 0.0f : __uint_as_float(e2)) : 0.0f;
-          if (c + 16 >= cbeg + ncol) {  // the accumulator is read: release it
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars.dempty[bi]);
-          }
-          {
-            float *mine = tiles + part * kXchFloats + lane * kXchPitch;
-            const bool sh = PAIR && (quarter & 1);  // tap b's sums sit one position to the right
-#pragma unroll
-            for (int t = 0; t < 16; ++t) mine[t] = sh ? v[t + 1] : v[t];
-          }
-          if (kAhead && c + 16 < cbeg + ncol) issue(c + 16);
-          named_sync(bar_id, bar_count);  // every part of the chunk is in place
-          // this warp's share: the parts of its filters, all loaded before the
-          // barrier that lets the group overwrite the tiles
-          float w[16];
-          int t0, fl;
-          if (p.vec4) {
-            // lane -> (filter 8*i + lane/4, positions 4*(lane%4) .. +3), i in the share
-            t0 = 4 * (lane & 3);
-            fl = lane >> 2;
-#pragma unroll
-            for (int k = 0; k < 4 / G; ++k)
-#pragma unroll
-              for (int q = 0; q < G; ++q)
-#pragma unroll
-                for (int e = 0; e < 4; ++e)
-                  w[(k * G + q) * 4 + e] = tiles[q * kXchFloats + (8 * (part * (4 / G) + k) + fl) * kXchPitch + t0 + e];
-          } else {
-            // lane -> (filter 2*i + lane/16, position lane%16), i in the share
-            t0 = lane & 15;
-            fl = lane >> 4;
-#pragma unroll
-            for (int k = 0; k < 16 / G; ++k)
-#pragma unroll
-              for (int q = 0; q < G; ++q)
-                w[k * G + q] = tiles[q * kXchFloats + (2 * (part * (16 / G) + k) + fl) * kXchPitch + t0];
-          }
-          named_sync(bar_id, bar_count);  // the tiles may be rewritten
-          const int Gp = p0 + c + t0;
-          const int Y = Gp / p.P, X = Gp - Y * p.P;
-          const bool ok = Y < ohv && X < bw && c + t0 < limit;
-          if (p.vec4) {
-            float *yo = ybase0 + (size_t)Y * ors + X;  // up == 1 here
-#pragma unroll
-            for (int k = 0; k < 4 / G; ++k) {
-              const int f = 8 * (part * (4 / G) + k) + fl;
-              float o[4];
-#pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                float acc = w[(k * G) * 4 + e];
-#pragma unroll
-                for (int q = 1; q < G; ++q) acc = acc + w[(k * G + q) * 4 + e];  // parts in order
-                o[e] = relu ? fmaxf(acc, 0.0f) : acc;
-              }
-              if (ok && fb + f < g.groups)
-                *reinterpret_cast<float4 *>(yo + (size_t)f * opl) = make_float4(o[0], o[1], o[2], o[3]);
-            }
-          } else {
-            float *yo = ybase0 + (size_t)Y * ors + (size_t)X * p.up;
-#pragma unroll
-            for (int k = 0; k < 16 / G; ++k) {
-              const int f = 2 * (part * (16 / G) + k) + fl;
-              float acc = w[k * G];
-#pragma unroll
-              for (int q = 1; q < G; ++q) acc = acc + w[k * G + q];  // parts in order
-              if (relu) acc = fmaxf(acc, 0.0f);
-              if (ok && fb + f < g.groups) yo[(size_t)f * opl] = acc;
-            }
-          }
-        }
+        // last segment: out = S (+ R) for every part of each filter
+        store_tile_columns<TERMS, PAIR>(p, it, sc, rc, first, cbeg, ncol, tiles, bar_id, quarter, part, lane,
+                                        &bars.dempty[bi]);
       }
     }
     if (failed) *abort_flag = 1;

@@ -1,7 +1,10 @@
 // Fused filter-bank convolution on the tcgen05 tensor cores, split BF16:
 // ProjectFrameBlockReduceSum / BackProjectFrameBlockReduceSum
 // (ConvolveHyperKernel.scala:153-199, 319-340, 574-645), every border policy
-// (:235-317), DownsampleOutput(1, 2) (:205-223), any field width.
+// (:235-317), DownsampleOutput(1, 2) (:205-223), UpsampleInput(2-4)
+// (:206-212, 405-459, as one sub-filter per output phase), any field width.
+// Banks of at most 32 filters put two taps of a filter row into each MMA
+// (paired taps: tap b's sums are read one grid position to the right).
 //
 // GEMM view, per image b and block of 64 filters:
 //   D[filter k][position p] = sum over (plane c, tap t) F[k][c, t] * X[c][p + off(t)]
@@ -39,11 +42,13 @@
 //               (zero, clamp, cyclic), split into bf16 terms, stored in the
 //               K-major core-matrix layout [plane group][position][8 planes];
 //               two buffers, so the next block is converted while the
-//               current one is multiplied.
+//               current one is multiplied.  Then they store half of the
+//               CTA's last tile with the epilogue warps.
 //   warp 8      MMA issuer (one elected lane): per (tile, plane block, tap):
 //               KS k-steps x nmma MMAs, A = filter chunk stage, B = halo.
 //   warp 9      loader (one lane): bulk copies of the pre-packed filter
-//               chunks (nb, plane block, tap) into a ring of stages.
+//               chunks (nb, plane block, tap) into a ring of stages, one copy
+//               per stage of several taps.
 //   warps 10-17 epilogue, two per tensor-memory lane quarter (alternate
 //               column halves): promotion adds, then per 16-column chunk the
 //               warps holding one filter block's parts write them to shared

@@ -671,6 +671,80 @@ def graph_workload(precision):
     }
 
 
+def circuit_bench(steps=200):
+    """A ComputeGraph that is a DAG, not a chain: two residual blocks
+    (conv+ReLU, conv, add the block's input, ReLU) at B=16, 64 planes, 64x64,
+    3x3, split BF16, stepped as one kernel circuit (a CUDA-graph replay over
+    shared buffers) and, beside it, node by node from the host (each
+    convolution through cct_conv_run, the adds and ReLUs as torch ops)."""
+    import numpy as np
+    import torch
+    from cctconv import _lib
+    from cctconv import circuit as K
+
+    B, C, H, W = 16, 64, 64, 64
+    d1 = _lib.new_desc(image_rows=H, image_cols=W, image_planes=B * C, filter_rows=3, filter_cols=3,
+                       filter_planes=C * C, batch_size=B, orientation=_lib.CROSS_CORRELATION,
+                       vector_mode=_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, precision=_lib.PREC_BF16X3,
+                       flags=_lib.FLAG_RELU)
+    d2 = _lib.new_desc(image_rows=H, image_cols=W, image_planes=B * C, filter_rows=3, filter_cols=3,
+                       filter_planes=C * C, batch_size=B, orientation=_lib.CROSS_CORRELATION,
+                       vector_mode=_lib.PROJECT_FRAME_BLOCK_REDUCE_SUM, precision=_lib.PREC_BF16X3)
+    nodes = [K.conv(0, d1), K.conv(1, d2), K.add(2, 0), K.relu(3),
+             K.conv(4, d1), K.conv(5, d2), K.add(6, 4), K.relu(7)]
+    circ = K.Circuit([(H, W, B * C)], nodes, outputs=[8])
+    rng = np.random.default_rng(6)
+    fs = {i: (rng.standard_normal((C * C, 3, 3)) * np.sqrt(2.0 / (C * 9))).astype(np.float32) for i in (0, 1, 4, 5)}
+    for i, f in fs.items():
+        circ.set_filter(i, f)
+    circ.field(0).uniform_(-1, 1)
+    stream = torch.cuda.current_stream().cuda_stream
+    gflop = 4 * 2.0 * B * C * H * W * C * 9 / 1e9
+
+    def timed(fn, n):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(n):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    ms_circuit = timed(lambda: circ.step(1, stream), steps)
+    # node by node from the host: the same plans and the same arithmetic
+    plans = {i: _lib.Plan(nodes[i].conv) for i in (0, 1, 4, 5)}
+    for i, pl in plans.items():
+        pl.set_static_filter(fs[i].ctypes.data)
+    x = circ.field(0).reshape(B * C, H, W).clone()
+    t = [torch.empty_like(x) for _ in range(3)]
+
+    def host_step():
+        plans[0].run(x.data_ptr(), 0, t[0].data_ptr(), stream)
+        plans[1].run(t[0].data_ptr(), 0, t[1].data_ptr(), stream)
+        torch.clamp_min(t[1].add_(x), 0.0, out=t[2])
+        plans[4].run(t[2].data_ptr(), 0, t[0].data_ptr(), stream)
+        plans[5].run(t[0].data_ptr(), 0, t[1].data_ptr(), stream)
+        torch.clamp_min(t[1].add_(t[2]), 0.0, out=t[0])
+
+    ms_host = timed(host_step, steps)
+    circ.step(1, stream)
+    host_step()
+    torch.cuda.synchronize()
+    same = bool(torch.equal(circ.field(8).reshape(B * C, H, W), t[0]))
+    nb, nbytes = circ.buffers()
+    out = {"config": {"workload": f"2 residual blocks, B={B}, {C} planes, {H}x{W}, 3x3, BF16X3, 8 nodes"},
+           "circuit_ms_per_step": round(ms_circuit, 4), "GFLOP/s": round(gflop / ms_circuit * 1e3, 1),
+           "host_dispatch_ms_per_step": round(ms_host, 4), "same_result_bits": same,
+           "buffers": nb, "fields": 1 + len(nodes), "buffer_MB": round(nbytes / 1e6, 1)}
+    for pl in plans.values():
+        pl.close()
+    circ.close()
+    return out
+
+
 def serve_requests(n, seed=5):
     """n seeded request specs: side log-uniform in [32, 1024], filter size
     from {3,5,7,9}, planes from {1,4,16,64}, filters from {1,16,64}."""
@@ -1108,6 +1182,7 @@ def main():
         suite["fft_convolve"] = sub_result(fft_workload, sub_steps, sub_warm, pg, world, peaks, peak_kind)
         suite["graph_stack"] = sub_result(lambda: graph_workload(args.precision), max(args.steps // 2, 5),
                                           sub_warm, pg, world, peaks, peak_kind)
+        suite["circuit_residual"] = circuit_bench()
         suite["serving"] = serve_suite(args)
 
     if rank != 0:

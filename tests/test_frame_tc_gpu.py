@@ -225,3 +225,44 @@ def test_tc_partial_last_wave_two_plane_blocks(mode, relu):
     check(a, od, x, f, relu=relu)
     b = run_tc(od, x, f, flags=flags)
     assert np.array_equal(a, b)
+
+
+def _random_cases(n, seed):
+    """Seeded random shapes over every border, both directions, down 2 and
+    up 2/3, both precisions, with and without ReLU."""
+    import random
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        border = rng.choice([O.ZERO, O.CLAMP, O.CYCLIC, O.VALID, O.FULL])
+        odd = border in (O.ZERO, O.CLAMP, O.CYCLIC)
+        R = rng.choice([1, 3, 5] if odd else [1, 2, 3, 4, 5])
+        samp = rng.choice(["none", "none", "down", "up"])
+        if samp == "up" and border == O.CLAMP:
+            border = O.ZERO  # integrated upsampling with BorderClamp is refused
+        H, W = rng.randint(max(R, 2), 40), rng.randint(max(R, 2), 44)
+        if samp == "down":
+            cr = R - 1 if border == O.VALID else (1 - R if border == O.FULL else 0)
+            H += (H - cr) % 2
+            W += (W - cr) % 2
+        out.append((H, W, rng.randint(1, 2), rng.randint(1, 40), rng.randint(1, 80), R, border,
+                    {"none": (O.NOSAMPLE, 1), "down": (O.DOWN, 2), "up": (O.UP, rng.choice([2, 3]))}[samp],
+                    rng.random() < 0.5, rng.random() < 0.25, rng.random() < 0.3))
+    return out
+
+
+@pytest.mark.parametrize("H,W,B,C,K,R,border,samp,back,x6,relu", _random_cases(40, 11))
+def test_tc_random_shapes(H, W, B, C, K, R, border, samp, back, x6, relu):
+    rng = np.random.default_rng(H * 7919 + W * 31 + C * 3 + K)
+    sampling, step = samp
+    if back:
+        planes, orient, mode = B * K, O.CONV, O.BACKPROJECT_REDUCE
+    else:
+        planes, orient, mode = B * C, O.XCORR, O.PROJECT_REDUCE
+    od = O.make_desc(H, W, R, R, planes=planes, f_planes=K * C, batch=B, border=border,
+                     orient=orient, sampling=sampling, step=step, mode=mode)
+    x = rng.standard_normal((planes, H, W)).astype(np.float32)
+    f = (rng.standard_normal((K * C, R, R)) * np.sqrt(2.0 / (C * R * R))).astype(np.float32)
+    prec = _lib.PREC_BF16X6 if x6 else _lib.PREC_BF16X3
+    y = run_tc(od, x, f, flags=_lib.FLAG_RELU if relu else 0, precision=prec)
+    check(y, od, x, f, relu=relu, tol=X6_TOL if x6 else TOL)

@@ -241,6 +241,462 @@ __global__ void fa_tc_reduce(const __grid_constant__ FaTcParams p, float *__rest
   }
 }
 
+// ---------------------------------------------------------------------------
+// Gradient-planes form (fa_bank_kernel), used when the rows suit TMA (widths
+// multiples of 4, 16-byte aligned fields) and a result row block fits:
+// OH * CB <= 160 accumulator columns for a plane block CB of 8..64.
+//
+// For a result column s the reduction over gradient columns j reads image
+// column j + s, so with s fixed:
+//   D_s[l][(r, c)] = sum_(b, i, j) g'[b*L + l](i, j) * x[b*C + c](r + i, s + j)
+// is a GEMM with rows m = gradient plane l (64 per block), columns
+// n = (result row r, image plane c) and the reduction k = (b, i, j).  A
+// reduction chunk is 16 gradient columns j0..j0+15 of gradient row i of image
+// b.  Its B operand is the image rows i..i+OH-1 at columns j0+s..: OH
+// consecutive [CB planes][16 columns] row tiles, so one stage's B is a run of
+// image-row tiles that every chunk of the stage reads at its own offset, and
+// the gradient (A) is converted once per chunk for two result columns (a CTA
+// serves the columns s0 and s0 + 1, one accumulator each).
+// Split BF16: a chunk's A1 (tensor memory) holds Gh in rows 0-63 and Gl in
+// rows 64-127, A2 the same halves swapped; A1 x Xh + A2 x Xl leaves
+// Gh*Xh + Gl*Xl in accumulator rows 0-63 and Gl*Xh + Gh*Xl in rows 64-127,
+// added after the reduction, so the small products never meet the large sum
+// in the tensor core's accumulation.  Rows of planes past L and columns of
+// planes past C hold other images' data (finite values) and are never
+// stored; gradient columns outside 0..Wg-1 come from TMA's zero fill.
+//
+// Warps 0-15 convert (fp32 staging -> A in tensor memory, B in shared
+// memory), warp 16 issues the MMAs, warp 17 issues the TMA loads of the fp32
+// staging: a gradient box [20 columns][7 rows][64 planes] and an image box
+// [20 columns][xrows][CB planes].  Their plane pitches are odd numbers of
+// 16-byte units, so the converters' float4 reads are conflict-free.  B
+// layout: [k group][row tile][8-row group][8 rows][16 B], 8-row groups
+// adjacent, which the tensor core reads at its full rate.  Each CTA reduces
+// a contiguous range of chunks, adds its two row halves and stores its
+// partial sums; fa_bank_reduce adds them in a fixed order.
+constexpr int kFbConvWarps = 16;
+constexpr int kFbConvThreads = 32 * kFbConvWarps;
+constexpr int kFbMmaWarp = 16;
+constexpr int kFbLoadWarp = 17;
+constexpr int kFbThreads = 32 * 18;
+constexpr int kFbChunks = 6;                    // chunks per stage
+constexpr int kFbGCols = 20, kFbGRows = 7;      // gradient box (odd plane pitch in 16-byte units)
+constexpr int kFbXCols = 20;                    // image box columns: s0 % 4 + 1 + 15 < 20
+constexpr int kFbLB = 64;                       // gradient planes per block
+constexpr int kFbMaxN = 160;                    // accumulator columns per result column
+constexpr int kFbAcol = 2 * kFbMaxN;            // first A column in tensor memory
+constexpr uint32_t kFbGBytes = kFbGCols * kFbGRows * kFbLB * 4;
+static_assert(kFbAcol + 2 * kFbChunks * 16 <= 512, "fa_bank tensor memory");
+static_assert(kFbGRows > kFbChunks && (kFbGCols / 4 * kFbGRows) % 2 == 1, "fa_bank gradient box");
+
+struct FaBankParams {
+  int H, W, Hg, Wg, OH, OW, C, L, B;
+  int CB, cb_log2, N, xrows, rows_max, cblocks, lblocks, JB, nch, S1;
+  uint32_t kg_bytes, term_bytes, bop_bytes, xbox_bytes, stg_bytes;
+  size_t smem;
+  float *part;  // [OW][C][OH][2*S1][lblocks*64]
+  unsigned *err;
+};
+
+struct FbStage {
+  int b, jb, i, n;
+};
+
+__device__ __forceinline__ FbStage fb_stage(const FaBankParams &p, int q, int q1) {
+  FbStage st;
+  const int t = q / p.Hg;
+  st.i = q - t * p.Hg;
+  st.jb = t % p.JB;
+  st.b = t / p.JB;
+  st.n = min(min(kFbChunks, q1 - q), p.Hg - st.i);
+  return st;
+}
+
+// B: image row tiles t < nrows; item (t, kg, c) with c fastest (a
+// quarter-warp reads 8 planes: conflict-free, and writes 128 contiguous
+// bytes); one 16-byte core row of each term for each result column, from
+// box column 8*kg + D + sh (D = s0 % 4, uniform).
+template <int D>
+__device__ __forceinline__ void fb_convert_b(const FaBankParams &p, const float *xbox, uint8_t *bbase, int nitems,
+                                             int nsh, int tid) {
+  for (int it = tid; it < nitems; it += kFbConvThreads) {
+    const int c = it & (p.CB - 1), tk = it >> p.cb_log2;
+    const int kg = tk & 1, t = tk >> 1;
+    const float4 *src = reinterpret_cast<const float4 *>(xbox + ((size_t)c * p.xrows + t) * kFbXCols + 8 * kg);
+    float w[12];
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const float4 t4 = src[v];
+      w[4 * v] = t4.x;
+      w[4 * v + 1] = t4.y;
+      w[4 * v + 2] = t4.z;
+      w[4 * v + 3] = t4.w;
+    }
+    uint8_t *dst = bbase + (uint32_t)kg * p.kg_bytes + ((uint32_t)t * p.CB + c) * 16;
+#pragma unroll
+    for (int sh = 0; sh < 2; ++sh) {
+      if (sh < nsh) {
+        uint32_t h[4], l[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) split_bf16x2(w[D + sh + 2 * v], w[D + sh + 2 * v + 1], h[v], l[v]);
+        uint8_t *d = dst + (size_t)(2 * sh) * p.term_bytes;
+        *reinterpret_cast<uint4 *>(d) = make_uint4(h[0], h[1], h[2], h[3]);
+        *reinterpret_cast<uint4 *>(d + p.term_bytes) = make_uint4(l[0], l[1], l[2], l[3]);
+      }
+    }
+  }
+}
+
+template <bool CONV>
+__global__ void __launch_bounds__(kFbThreads, 1)
+    fa_bank_kernel(const __grid_constant__ FaBankParams p, const __grid_constant__ CUtensorMap gmap,
+                   const __grid_constant__ CUtensorMap xmap) {
+  // 2 fp32 staging slots [gradient box | image box], then 2 B operand slots
+  // [result column][hi | lo][k group][row tiles]
+  extern __shared__ __align__(1024) uint8_t smem[];
+  __shared__ __align__(8) uint64_t fp_full[2], fp_empty[2], op_full[2], op_empty[2], done;
+  __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // CTA: (plane block, gradient block, result-column group, split); group g
+  // serves columns 2g and 2g + 1 (the last may have one) with w_g * S1 splits
+  int bid = blockIdx.x;
+  const int e = bid % (p.OW * p.S1);
+  bid /= p.OW * p.S1;
+  const int cblk = bid % p.cblocks, lblk = bid / p.cblocks;
+  const int grp = e / (2 * p.S1), sp = e - grp * 2 * p.S1;
+  const int s0 = 2 * grp, nsh = min(2, p.OW - s0);
+  const int nsplit = nsh * p.S1;
+  const int q0 = (int)((long long)sp * p.nch / nsplit), q1 = (int)((long long)(sp + 1) * p.nch / nsplit);
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 2; ++k) {
+      mbar_init(&fp_full[k], 1);              // loader expect_tx
+      mbar_init(&fp_empty[k], kFbConvWarps);  // one arrival per converter warp
+      mbar_init(&op_full[k], kFbConvWarps);
+      mbar_init(&op_empty[k], 1);             // MMA commit
+    }
+    mbar_init(&done, 1);
+    abort_flag = 0;
+    fence_barrier_init();
+  }
+  if (warp == kFbMmaWarp) tmem_alloc(&tmem_slot, 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  grid_dependency_wait();  // launched with programmatic serialisation: global memory only after this
+  allow_dependent_launch();
+  volatile int *abort = &abort_flag;
+  uint8_t *ops = smem + 2 * (size_t)p.stg_bytes;
+  bool failed = false;
+
+  if (warp < kFbConvWarps) {
+    // ------------------------------------------------------------ converters
+    const int quarter = warp & 3, par = warp >> 2;  // lane quarter, chunk phase (0-3)
+    const int lloc = (quarter & 1) * 32 + lane, half = quarter >> 1;
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    const int dsh = s0 & 3;  // image box column of result column s0 at gradient column j0
+    int u = 0;
+    for (int q = q0; q < q1; ++u) {
+      const FbStage st = fb_stage(p, q, q1);
+      const int slot = u & 1;
+      const uint32_t ph = (uint32_t)(u >> 1) & 1;
+      if (*abort || !mbar_wait(&fp_full[slot], ph, p.err) ||
+          (u >= 2 && !mbar_wait(&op_empty[slot], ph ^ 1, p.err))) {
+        failed = true;
+        break;
+      }
+      const uint8_t *stg = smem + (size_t)slot * p.stg_bytes;
+      // A: chunks par, par + 4 of the stage, this lane's gradient plane.  The
+      // box row of gradient row i + k is k (convolution: the box starts at row
+      // Hg - i - 7 and column Wg - 16 - j0, read backwards: row 6 - k, column 15 - kk)
+      for (int k = par; k < st.n; k += 4) {
+        const float4 *src = reinterpret_cast<const float4 *>(stg) +
+                            ((size_t)lloc * kFbGRows + (CONV ? kFbGRows - 1 - k : k)) * (kFbGCols / 4);
+        float v[16];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const float4 t = src[w];
+          if (CONV) {
+            v[15 - 4 * w] = t.x;
+            v[14 - 4 * w] = t.y;
+            v[13 - 4 * w] = t.z;
+            v[12 - 4 * w] = t.w;
+          } else {
+            v[4 * w] = t.x;
+            v[4 * w + 1] = t.y;
+            v[4 * w + 2] = t.z;
+            v[4 * w + 3] = t.w;
+          }
+        }
+        uint32_t hi[8], lo[8];
+#pragma unroll
+        for (int w = 0; w < 8; ++w) split_bf16x2(v[2 * w], v[2 * w + 1], hi[w], lo[w]);
+        const uint32_t a1 = tmem + lane_base + kFbAcol + (uint32_t)(slot * kFbChunks + k) * 16;
+        if (half == 0) {
+          tmem_st8(a1, hi);
+          tmem_st8(a1 + 8, lo);
+        } else {
+          tmem_st8(a1, lo);
+          tmem_st8(a1 + 8, hi);
+        }
+      }
+      const float *xbox = reinterpret_cast<const float *>(stg + kFbGBytes);
+      uint8_t *opb = ops + (size_t)slot * p.bop_bytes;
+      const int nitems = (st.n + p.OH - 1) * 2 * p.CB;
+      switch (dsh) {
+        case 0: fb_convert_b<0>(p, xbox, opb, nitems, nsh, threadIdx.x); break;
+        case 1: fb_convert_b<1>(p, xbox, opb, nitems, nsh, threadIdx.x); break;
+        case 2: fb_convert_b<2>(p, xbox, opb, nitems, nsh, threadIdx.x); break;
+        default: fb_convert_b<3>(p, xbox, opb, nitems, nsh, threadIdx.x); break;
+      }
+      // the tensor core reads A (tensor memory) and B (async proxy)
+      tc_wait_st();
+      fence_proxy_async_smem();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) {
+        mbar_arrive(&fp_empty[slot]);
+        mbar_arrive(&op_full[slot]);
+      }
+      q += st.n;
+    }
+    if (failed) *abort = 1;
+    // -------------------------------------------------------------- epilogue
+    // Rows 64-127 (the small products) go through shared memory (the fp32
+    // staging, idle now: every load was consumed) to the warps holding rows
+    // 0-63, which add and store.
+    bool bad = failed || *abort != 0;
+    if (!bad) bad = !mbar_wait(&done, 0, p.err);
+    bad = named_sync_or(1, kFbConvThreads, bad);
+    float *xch = reinterpret_cast<float *>(smem);  // [result column][column][64 lanes]
+    if (!bad) {
+      tc_fence_after();
+      if (half == 1) {
+        for (int sh = 0; sh < nsh; ++sh)
+          for (int c0 = par * 16; c0 < p.N; c0 += 64) {
+            uint32_t v[16];
+            tmem_ld16(tmem + lane_base + (uint32_t)(sh * p.N + c0), v);
+            tc_wait_ld();
+#pragma unroll
+            for (int k = 0; k < 16; ++k) xch[((size_t)sh * p.N + c0 + k) * 64 + lloc] = __uint_as_float(v[k]);
+          }
+      }
+    }
+    named_sync(1, kFbConvThreads);
+    if (!bad && half == 0) {
+      const int Lpad = p.lblocks * kFbLB;
+      for (int sh = 0; sh < nsh; ++sh) {
+        // partial sums of (s, c, r) from all splits are one contiguous run: [s][c][r][split][l]
+        float *dst = p.part + (((size_t)(s0 + sh) * p.C) * p.OH * 2 * p.S1 + sp) * Lpad + lblk * kFbLB + lloc;
+        for (int c0 = par * 16; c0 < p.N; c0 += 64) {
+          uint32_t v[16];
+          tmem_ld16(tmem + lane_base + (uint32_t)(sh * p.N + c0), v);
+          tc_wait_ld();
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const int n = c0 + k, r = n >> p.cb_log2, cg = cblk * p.CB + (n & (p.CB - 1));
+            const float sum = __uint_as_float(v[k]) + xch[((size_t)sh * p.N + n) * 64 + lloc];
+            // an empty chunk range (more splits than chunks) contributes zeros
+            if (cg < p.C) dst[((size_t)cg * p.OH + r) * 2 * p.S1 * Lpad] = q0 < q1 ? sum : 0.0f;
+          }
+        }
+      }
+    }
+  } else if (warp == kFbMmaWarp) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16_f32(128, p.N);
+      const uint64_t bt = smem_desc_kmajor(0, p.kg_bytes, 128);
+      const uint32_t b_hi = (uint32_t)(bt >> 32), b_lo = (uint32_t)bt;
+      // The issuing thread's own latency bounds the MMA rate, so the loop
+      // keeps running 32-bit descriptor words and no per-MMA branching.
+      const uint32_t ops16 = smem_u32(ops) >> 4;
+      const uint32_t cb16 = (uint32_t)p.CB, term16 = p.term_bytes >> 4;  // a row tile: CB rows of 16 bytes
+      const uint32_t d0 = tmem, d1 = tmem + (uint32_t)p.N;
+      const bool two = nsh == 2;
+      uint32_t acc = 0;
+      int u = 0;
+      for (int q = q0; q < q1; ++u) {
+        const FbStage st = fb_stage(p, q, q1);
+        const int slot = u & 1;
+        if (*abort || !mbar_wait(&op_full[slot], (uint32_t)(u >> 1) & 1, p.err)) {
+          failed = true;
+          break;
+        }
+        tc_fence_after();
+        uint32_t a1 = tmem + kFbAcol + (uint32_t)(slot * kFbChunks) * 16;
+        uint32_t bw = b_lo + ops16 + ((uint32_t)slot * p.bop_bytes >> 4);
+        for (int k = 0; k < st.n; ++k, a1 += 16, bw += cb16) {
+          mma_bf16_ts(d0, a1, desc_word(b_hi, bw), idesc, acc);
+          mma_bf16_ts(d0, a1 + 8, desc_word(b_hi, bw + term16), idesc, 1u);
+          if (two) {
+            mma_bf16_ts(d1, a1, desc_word(b_hi, bw + 2 * term16), idesc, acc);
+            mma_bf16_ts(d1, a1 + 8, desc_word(b_hi, bw + 3 * term16), idesc, 1u);
+          }
+          acc = 1u;
+        }
+        tc_commit(&op_empty[slot]);  // frees the stage once its MMAs are done
+        q += st.n;
+      }
+      tc_commit(&done);
+      if (failed) *abort = 1;
+      mbar_wait(&done, 0, p.err);  // every MMA retired before the tensor memory is freed
+    }
+    __syncwarp();
+  } else if (warp == kFbLoadWarp) {
+    // --------------------------------------------------------------- loader
+    if (lane == 0) {
+      int u = 0;
+      for (int q = q0; q < q1; ++u) {
+        const FbStage st = fb_stage(p, q, q1);
+        const int slot = u & 1;
+        if (*abort || (u >= 2 && !mbar_wait(&fp_empty[slot], ((uint32_t)(u >> 1) & 1) ^ 1, p.err))) {
+          *abort = 1;
+          break;
+        }
+        uint8_t *gdst = smem + (size_t)slot * p.stg_bytes;
+        const int j0 = st.jb * 16;
+        mbar_arrive_expect_tx(&fp_full[slot], kFbGBytes + p.xbox_bytes);
+        tma_load_3d(gdst, &gmap, &fp_full[slot], CONV ? p.Wg - 16 - j0 : j0, CONV ? p.Hg - st.i - kFbGRows : st.i,
+                    st.b * p.L + lblk * kFbLB);
+        tma_load_3d(gdst + kFbGBytes, &xmap, &fp_full[slot], j0 + (s0 & ~3), st.i, st.b * p.C + cblk * p.CB);
+        q += st.n;
+      }
+    }
+    __syncwarp();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == kFbMmaWarp) tmem_dealloc(tmem, 512);
+}
+
+// out[l*C + c](r, s) = the CTAs' partial sums for (s, c, r, l) in a fixed
+// order.  A block serves one (s, c, r), whose partial sums are one
+// contiguous run [split][planes]: thread (quad, k) loads four planes of every
+// sixteenth split from k (all its loads in flight at once), and the sixteen
+// sums of each plane are added in a fixed tree.
+__global__ void __launch_bounds__(256) fa_bank_reduce(const __grid_constant__ FaBankParams p, float *__restrict__ y) {
+  __shared__ float4 red[16][17];
+  grid_dependency_wait();
+  const int Lpad = p.lblocks * kFbLB, quads = Lpad / 4;
+  const int k = threadIdx.x >> 4, lq4 = threadIdx.x & 15;
+  const int nblk = p.OW * p.C * p.OH * ((quads + 15) / 16);
+  for (int bi = blockIdx.x; bi < nblk; bi += gridDim.x) {
+    const int qb = bi % ((quads + 15) / 16), scr = bi / ((quads + 15) / 16);  // scr = (s * C + c) * OH + r
+    const int r = scr % p.OH, sc = scr / p.OH;
+    const int cg = sc % p.C, s = sc / p.C;
+    const int nsplit = (s / 2 * 2 + 1 < p.OW ? 2 : 1) * p.S1;
+    const int quad = qb * 16 + lq4;
+    const float4 *q = reinterpret_cast<const float4 *>(p.part + (size_t)scr * 2 * p.S1 * Lpad) + quad;
+    float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (quad < quads) {
+      for (int base = k; base < nsplit; base += 16 * 8) {
+        float4 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+          v[j] = base + 16 * j < nsplit ? q[(size_t)(base + 16 * j) * quads] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          acc.x += v[j].x;
+          acc.y += v[j].y;
+          acc.z += v[j].z;
+          acc.w += v[j].w;
+        }
+      }
+    }
+    red[k][lq4] = acc;
+    __syncthreads();
+    if (threadIdx.x < 64) {
+      // plane 4 * (qb * 16 + t / 4) + t % 4: the sixteen split lanes in a fixed tree
+      const int t = threadIdx.x, qq = t >> 2, comp = t & 3;
+      float w[16];
+#pragma unroll
+      for (int kk = 0; kk < 16; ++kk) {
+        const float4 a = red[kk][qq];
+        w[kk] = comp == 0 ? a.x : comp == 1 ? a.y : comp == 2 ? a.z : a.w;
+      }
+#pragma unroll
+      for (int h = 8; h >= 1; h >>= 1)
+#pragma unroll
+        for (int kk = 0; kk < h; ++kk) w[kk] += w[kk + h];
+      const int l = 4 * (qb * 16 + qq) + comp;
+      if (l < p.L) y[((size_t)l * p.C + cg) * p.OH * p.OW + (size_t)r * p.OW + s] = w[0];
+    }
+    __syncthreads();
+  }
+}
+
+// The gradient-planes form's plan, or false when the shape does not suit it.
+bool make_bank_params(const ConvGeom &g, int sms, FaBankParams *out) {
+  FaBankParams p{};
+  p.Hg = g.R;
+  p.Wg = g.S;
+  p.OH = g.OH;
+  p.OW = g.OW;
+  p.H = g.H;
+  p.W = g.W;
+  p.C = g.n;
+  p.L = g.groups;
+  p.B = g.batch;
+  if ((p.W & 3) || (p.Wg & 3) || p.OH < 1 || p.OW < 1 || p.L < 1 || p.C < 1) return false;
+  const size_t budget = 225 * 1024;
+  // plane block (a power of two): the fewest blocks, then the smallest block
+  bool found = false;
+  int best_blocks = 0;
+  for (int lg = 3; lg <= 6; ++lg) {
+    const int cb = 1 << lg;
+    if (cb * p.OH > kFbMaxN || (cb * p.OH) % 16) continue;
+    const int rows_max = kFbChunks + p.OH - 1;
+    const int xrows = rows_max | 1;  // odd: the image staging's plane pitch is an odd number of 16-byte units
+    const uint32_t xbox = (uint32_t)kFbXCols * xrows * cb * 4;
+    const uint32_t stg = kFbGBytes + xbox;  // gradient box + image box
+    const uint32_t kgb = (uint32_t)rows_max * cb * 16;  // one k group of a term's row tiles
+    const uint32_t term = 2 * kgb;
+    const uint32_t bop = 4 * term;                      // two result columns x (hi, lo)
+    const size_t smem = 2 * (size_t)stg + 2 * (size_t)bop;
+    // the epilogue's exchange (two columns x N x 64 lanes) reuses the staging and operands
+    if (smem > budget || (size_t)2 * cb * p.OH * 64 * 4 > smem) continue;
+    const int nb = (p.C + cb - 1) / cb;
+    if (found && nb >= best_blocks) continue;
+    found = true;
+    best_blocks = nb;
+    p.CB = cb;
+    p.cb_log2 = lg;
+    p.N = cb * p.OH;
+    p.rows_max = rows_max;
+    p.xrows = xrows;
+    p.xbox_bytes = xbox;
+    p.stg_bytes = stg;
+    p.kg_bytes = kgb;
+    p.term_bytes = term;
+    p.bop_bytes = bop;
+    p.smem = smem;
+  }
+  if (!found || p.xrows > 256) return false;
+  p.cblocks = best_blocks;
+  p.lblocks = (p.L + kFbLB - 1) / kFbLB;
+  p.JB = (p.Wg + 15) / 16;
+  const long long nch = (long long)p.B * p.JB * p.Hg;
+  if (nch < 1 || nch > 0x3fffffffLL) return false;
+  p.nch = (int)nch;
+  const long long per_col = (long long)p.cblocks * p.lblocks * p.OW;
+  p.S1 = (int)std::max(1LL, std::min<long long>(sms / per_col, (p.nch + 1) / 2));
+  if (per_col * p.S1 > 0x7fffffffLL || (long long)p.OW * p.C * p.OH * p.lblocks * kFbLB * 2 * p.S1 > 0x7fffffffLL)
+    return false;
+  // more than 160 KB keeps one CTA per SM: its 512 tensor-memory columns are free
+  p.smem = std::max(p.smem, (size_t)160 * 1024);
+  *out = p;
+  return true;
+}
+
+size_t bank_workspace_bytes(const FaBankParams &p) {
+  return (size_t)2 * p.S1 * p.OW * p.C * p.OH * p.lblocks * kFbLB * sizeof(float);
+}
+
 FaTcParams make_params(const ConvGeom &g, int sms) {
   FaTcParams p{};
   p.Hg = g.R;
@@ -280,20 +736,59 @@ bool fa_tc_supported(const ConvGeom &g) {
 
 size_t fa_tc_workspace_bytes(const ConvGeom &g, int sms) {
   const FaTcParams p = make_params(g, sms);
-  return (size_t)p.splits * p.Lpad * p.Mpad * sizeof(float);
+  size_t bytes = (size_t)p.splits * p.Lpad * p.Mpad * sizeof(float);
+  FaBankParams bp;
+  if (make_bank_params(g, sms, &bp)) bytes = std::max(bytes, bank_workspace_bytes(bp));
+  return bytes;
 }
+
+namespace {
+
+int launch_fa_bank(FaBankParams p, bool conv, const float *x, const float *f, float *y, cudaStream_t st) {
+  CUtensorMap gmap, xmap;
+  int rc = encode_tensor_map_3d_box(&gmap, f, (uint64_t)p.Wg, (uint64_t)p.Hg, (uint64_t)p.B * p.L, kFbGCols,
+                                    kFbGRows, kFbLB);
+  if (rc) return rc;
+  rc = encode_tensor_map_3d_box(&xmap, x, (uint64_t)p.W, (uint64_t)p.H, (uint64_t)p.B * p.C, kFbXCols,
+                                (uint32_t)p.xrows, (uint32_t)p.CB);
+  if (rc) return rc;
+  auto kern = conv ? fa_bank_kernel<true> : fa_bank_kernel<false>;
+  rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem),
+                  "cudaFuncSetAttribute(fa_bank)");
+  if (rc) return rc;
+  const long long grid = (long long)p.cblocks * p.lblocks * p.OW * p.S1;
+  rc = launch_pdl(kern, dim3((unsigned)grid), dim3(kFbThreads), p.smem, st, "fa_bank_kernel launch", p, gmap, xmap);
+  if (rc) return rc;
+  const long long nblk = (long long)p.OW * p.C * p.OH * p.lblocks;  // < 2^31: the plan checks it
+  const int blocks = (int)std::min<long long>(nblk, 148LL * 16);
+  rc = launch_pdl(fa_bank_reduce, dim3(blocks), dim3(256), 0, st, "fa_bank_reduce launch", p, y);
+  if (rc) return rc;
+  count_launches(2);
+  return CCT_OK;
+}
+
+}  // namespace
 
 int launch_fa_tc(const ConvGeom &g, const float *x, const float *f, float *y, float *work, unsigned *err,
                  cudaStream_t st) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (!work) return set_error(CCT_EINVAL, "tensor-core FilterAdjoint needs plan workspace");
+  FaBankParams bp;
+  // TMA reads both fields: 16-byte aligned bases (row pitches are checked by
+  // the plan)
+  if (make_bank_params(g, sms, &bp) && (reinterpret_cast<uintptr_t>(x) & 15) == 0 &&
+      (reinterpret_cast<uintptr_t>(f) & 15) == 0) {
+    bp.part = work;
+    bp.err = err;
+    return launch_fa_bank(bp, g.orient == CCT_CONVOLUTION, x, f, y, st);
+  }
   FaTcParams p = make_params(g, sms);
   p.x = x;
   p.g = f;
   p.part = work;
   p.err = err;
-  if (!work) return set_error(CCT_EINVAL, "tensor-core FilterAdjoint needs plan workspace");
   const long long grid = (long long)p.mtiles * p.nblocks * p.splits;
   if (grid > 0x7fffffffLL) return set_error(CCT_ENOTSUP, "FilterAdjoint grid too large");
   // the stages need kStages * 2 * NT * 32 bf16 (32 KB at most); asking for 96 KB keeps

@@ -138,6 +138,12 @@ TC_CASES = [
     (5, 72, 20, 21, 16, 17, 3),     # L = 72: two column blocks; 4x5 results
     (1, 16, 9, 9, 1, 1, 5),         # 1x1 gradient: one pixel per chunk
     (7, 24, 40, 33, 33, 31, 1),     # one image, 8x3 results
+    # gradient-planes form (image and gradient widths multiples of 4)
+    (16, 40, 36, 40, 32, 36, 3),    # 5x5 results, a ragged 16-column gradient block
+    (70, 20, 13, 16, 9, 12, 2),     # three 32-plane blocks of the image
+    (8, 100, 20, 24, 16, 20, 2),    # two 64-plane gradient blocks
+    (12, 6, 6, 16, 6, 16, 2),       # a 1x1 result
+    (9, 4, 7, 20, 5, 16, 1),        # 3x5 results, fewer chunks than splits
 ]
 
 

@@ -265,6 +265,26 @@ int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols,
   return CCT_OK;
 }
 
+int encode_tensor_map_f32(CUtensorMap *map, const float *base, int rank, const uint64_t *dims,
+                          const uint64_t *strides, const uint32_t *box) {
+  EncodeFn fn = encode_fn();
+  if (!fn) return set_error(CCT_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  if (rank < 1 || rank > 5) return set_error(CCT_EINVAL, "tensor map rank %d", rank);
+  cuuint64_t d[5], st[4];
+  cuuint32_t b[5], e[5];
+  for (int i = 0; i < rank; ++i) {
+    d[i] = dims[i];
+    b[i] = box[i];
+    e[i] = 1;
+    if (i > 0) st[i - 1] = strides[i - 1];
+  }
+  CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (cuuint32_t)rank, (void *)base, d, st, b, e,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_error(CCT_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CCT_OK;
+}
+
 bool direct_tma_supported(const ConvGeom &g, const float *x) {
   if (g.terms != 1 || g.up != 1 || g.down != 1 || g.fup != 1) return false;
   if (g.border != CCT_BORDER_ZERO && g.border != CCT_BORDER_FULL && g.border != CCT_BORDER_VALID)

@@ -268,7 +268,8 @@ __global__ void fa_tc_reduce(const __grid_constant__ FaTcParams p, float *__rest
 // Warps 0-15 convert (fp32 staging -> A in tensor memory, B in shared
 // memory), warp 16 issues the MMAs, warp 17 issues the TMA loads of the fp32
 // staging: a gradient box [20 columns][7 rows][64 planes] and an image box
-// [20 columns][xrows][CB planes].  Their plane pitches are odd numbers of
+// [20 columns][xrows][CB planes], three stages deep (a box took ~3k cycles
+// to land).  Their plane pitches are odd numbers of
 // 16-byte units, so the converters' float4 reads are conflict-free.  B
 // layout: [k group][row tile][8-row group][8 rows][16 B], 8-row groups
 // adjacent, which the tensor core reads at its full rate.  Each CTA reduces
@@ -279,22 +280,24 @@ constexpr int kFbConvThreads = 32 * kFbConvWarps;
 constexpr int kFbMmaWarp = 16;
 constexpr int kFbLoadWarp = 17;
 constexpr int kFbThreads = 32 * 18;
-constexpr int kFbChunks = 6;                    // chunks per stage
-constexpr int kFbGCols = 20, kFbGRows = 7;      // gradient box (odd plane pitch in 16-byte units)
+constexpr int kFbChunks = 5;                    // chunks per stage
+constexpr int kFbStg = 3;                       // fp32 staging slots: a load has two stages to land
+constexpr int kFbGCols = 20, kFbGRows = 5;      // gradient box (odd plane pitch in 16-byte units)
 constexpr int kFbXCols = 20;                    // image box columns: s0 % 4 + 1 + 15 < 20
 constexpr int kFbLB = 64;                       // gradient planes per block
 constexpr int kFbMaxN = 160;                    // accumulator columns per result column
 constexpr int kFbAcol = 2 * kFbMaxN;            // first A column in tensor memory
 constexpr uint32_t kFbGBytes = kFbGCols * kFbGRows * kFbLB * 4;
 static_assert(kFbAcol + 2 * kFbChunks * 16 <= 512, "fa_bank tensor memory");
-static_assert(kFbGRows > kFbChunks && (kFbGCols / 4 * kFbGRows) % 2 == 1, "fa_bank gradient box");
+static_assert(kFbGRows >= kFbChunks && (kFbGCols / 4 * kFbGRows) % 2 == 1, "fa_bank gradient box");
 
 struct FaBankParams {
   int H, W, Hg, Wg, OH, OW, C, L, B;
-  int CB, cb_log2, N, xrows, rows_max, cblocks, lblocks, JB, nch, S1;
+  int CB, cb_log2, N, xrows, rows_max, cblocks, lblocks, JB, nch;
+  int npairs, P, Q, NS;  // column pairs; splits of a pair, of the lone column (odd OW); max(P, Q)
   uint32_t kg_bytes, term_bytes, bop_bytes, xbox_bytes, stg_bytes;
   size_t smem;
-  float *part;  // [OW][C][OH][2*S1][lblocks*64]
+  float *part;  // [OW][C][OH][NS][lblocks*64]
   unsigned *err;
 };
 
@@ -350,30 +353,34 @@ __device__ __forceinline__ void fb_convert_b(const FaBankParams &p, const float 
 template <bool CONV>
 __global__ void __launch_bounds__(kFbThreads, 1)
     fa_bank_kernel(const __grid_constant__ FaBankParams p, const __grid_constant__ CUtensorMap gmap,
-                   const __grid_constant__ CUtensorMap xmap) {
-  // 2 fp32 staging slots [gradient box | image box], then 2 B operand slots
+                   const __grid_constant__ CUtensorMap xmap, const __grid_constant__ CUtensorMap omap) {
+  // 3 fp32 staging slots [gradient box | image box], then 2 B operand slots
   // [result column][hi | lo][k group][row tiles]
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t fp_full[2], fp_empty[2], op_full[2], op_empty[2], done;
+  __shared__ __align__(8) uint64_t fp_full[kFbStg], fp_empty[kFbStg], op_full[2], op_empty[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   // CTA: (plane block, gradient block, result-column group, split); group g
-  // serves columns 2g and 2g + 1 (the last may have one) with w_g * S1 splits
+  // serves columns 2g and 2g + 1 with P splits, or (odd OW) the last column
+  // alone with Q splits
   int bid = blockIdx.x;
-  const int e = bid % (p.OW * p.S1);
-  bid /= p.OW * p.S1;
+  const int per_cl = p.npairs * p.P + p.Q;
+  const int e = bid % per_cl;
+  bid /= per_cl;
   const int cblk = bid % p.cblocks, lblk = bid / p.cblocks;
-  const int grp = e / (2 * p.S1), sp = e - grp * 2 * p.S1;
+  const int grp = e < p.npairs * p.P ? e / p.P : p.npairs, sp = e - grp * p.P;
   const int s0 = 2 * grp, nsh = min(2, p.OW - s0);
-  const int nsplit = nsh * p.S1;
+  const int nsplit = grp < p.npairs ? p.P : p.Q;
   const int q0 = (int)((long long)sp * p.nch / nsplit), q1 = (int)((long long)(sp + 1) * p.nch / nsplit);
 
   if (threadIdx.x == 0) {
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kFbStg; ++k) {
       mbar_init(&fp_full[k], 1);              // loader expect_tx
       mbar_init(&fp_empty[k], kFbConvWarps);  // one arrival per converter warp
+    }
+    for (int k = 0; k < 2; ++k) {
       mbar_init(&op_full[k], kFbConvWarps);
       mbar_init(&op_empty[k], 1);             // MMA commit
     }
@@ -389,7 +396,7 @@ __global__ void __launch_bounds__(kFbThreads, 1)
   grid_dependency_wait();  // launched with programmatic serialisation: global memory only after this
   allow_dependent_launch();
   volatile int *abort = &abort_flag;
-  uint8_t *ops = smem + 2 * (size_t)p.stg_bytes;
+  uint8_t *ops = smem + kFbStg * (size_t)p.stg_bytes;
   bool failed = false;
 
   if (warp < kFbConvWarps) {
@@ -401,17 +408,17 @@ __global__ void __launch_bounds__(kFbThreads, 1)
     int u = 0;
     for (int q = q0; q < q1; ++u) {
       const FbStage st = fb_stage(p, q, q1);
-      const int slot = u & 1;
+      const int slot = u & 1, sslot = u % kFbStg;
       const uint32_t ph = (uint32_t)(u >> 1) & 1;
-      if (*abort || !mbar_wait(&fp_full[slot], ph, p.err) ||
+      if (*abort || !mbar_wait(&fp_full[sslot], (uint32_t)(u / kFbStg) & 1, p.err) ||
           (u >= 2 && !mbar_wait(&op_empty[slot], ph ^ 1, p.err))) {
         failed = true;
         break;
       }
-      const uint8_t *stg = smem + (size_t)slot * p.stg_bytes;
+      const uint8_t *stg = smem + (size_t)sslot * p.stg_bytes;
       // A: chunks par, par + 4 of the stage, this lane's gradient plane.  The
       // box row of gradient row i + k is k (convolution: the box starts at row
-      // Hg - i - 7 and column Wg - 16 - j0, read backwards: row 6 - k, column 15 - kk)
+      // Hg - i - 5 and column Wg - 16 - j0, read backwards: row 4 - k, column 15 - kk)
       for (int k = par; k < st.n; k += 4) {
         const float4 *src = reinterpret_cast<const float4 *>(stg) +
                             ((size_t)lloc * kFbGRows + (CONV ? kFbGRows - 1 - k : k)) * (kFbGCols / 4);
@@ -458,52 +465,75 @@ __global__ void __launch_bounds__(kFbThreads, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) {
-        mbar_arrive(&fp_empty[slot]);
+        mbar_arrive(&fp_empty[sslot]);
         mbar_arrive(&op_full[slot]);
       }
       q += st.n;
     }
     if (failed) *abort = 1;
     // -------------------------------------------------------------- epilogue
-    // Rows 64-127 (the small products) go through shared memory (the fp32
-    // staging, idle now: every load was consumed) to the warps holding rows
-    // 0-63, which add and store.
+    // The CTA's partial sums are assembled in shared memory (idle now: every
+    // load was consumed and every MMA has retired) as TMA store boxes
+    // [result column][CB * OH (plane, row)][64 planes l]: the warps holding
+    // rows 0-63 (Gh*Xh + Gl*Xl) and those holding rows 64-127 (the small
+    // products) write two copies at once, all warps add them (float4), and
+    // one thread stores each column's box.
     bool bad = failed || *abort != 0;
     if (!bad) bad = !mbar_wait(&done, 0, p.err);
     bad = named_sync_or(1, kFbConvThreads, bad);
-    float *xch = reinterpret_cast<float *>(smem);  // [result column][column][64 lanes]
+    const int box_floats = p.CB * p.OH * kFbLB;
+    float *obox = reinterpret_cast<float *>(smem);               // rows 0-63, then the sums
+    float *sbox = obox + (size_t)2 * box_floats;                 // rows 64-127
     if (!bad) {
       tc_fence_after();
-      if (half == 1) {
-        for (int sh = 0; sh < nsh; ++sh)
-          for (int c0 = par * 16; c0 < p.N; c0 += 64) {
-            uint32_t v[16];
-            tmem_ld16(tmem + lane_base + (uint32_t)(sh * p.N + c0), v);
-            tc_wait_ld();
-#pragma unroll
-            for (int k = 0; k < 16; ++k) xch[((size_t)sh * p.N + c0 + k) * 64 + lloc] = __uint_as_float(v[k]);
-          }
-      }
-    }
-    named_sync(1, kFbConvThreads);
-    if (!bad && half == 0) {
-      const int Lpad = p.lblocks * kFbLB;
+      float *mine = half ? sbox : obox;
+      const int stride = p.OH * kFbLB;  // between planes c and c + 1 of one result row r
       for (int sh = 0; sh < nsh; ++sh) {
-        // partial sums of (s, c, r) from all splits are one contiguous run: [s][c][r][split][l]
-        float *dst = p.part + (((size_t)(s0 + sh) * p.C) * p.OH * 2 * p.S1 + sp) * Lpad + lblk * kFbLB + lloc;
         for (int c0 = par * 16; c0 < p.N; c0 += 64) {
           uint32_t v[16];
           tmem_ld16(tmem + lane_base + (uint32_t)(sh * p.N + c0), v);
           tc_wait_ld();
+          // columns n = c0..c0+15 = (r, c): box row c * OH + r; an empty chunk
+          // range (more splits than chunks) contributes zeros
+          float *o = mine + (size_t)sh * box_floats + lloc;
+          if (p.CB >= 16) {  // one result row per 16 columns
+            float *ob = o + ((size_t)(c0 & (p.CB - 1)) * p.OH + (c0 >> p.cb_log2)) * kFbLB;
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const int n = c0 + k, r = n >> p.cb_log2, cg = cblk * p.CB + (n & (p.CB - 1));
-            const float sum = __uint_as_float(v[k]) + xch[((size_t)sh * p.N + n) * 64 + lloc];
-            // an empty chunk range (more splits than chunks) contributes zeros
-            if (cg < p.C) dst[((size_t)cg * p.OH + r) * 2 * p.S1 * Lpad] = q0 < q1 ? sum : 0.0f;
+            for (int k = 0; k < 16; ++k) ob[k * stride] = q0 < q1 ? __uint_as_float(v[k]) : 0.0f;
+          } else {
+#pragma unroll
+            for (int k = 0; k < 16; ++k) {
+              const int n = c0 + k;
+              o[((size_t)(n & (p.CB - 1)) * p.OH + (n >> p.cb_log2)) * kFbLB] = q0 < q1 ? __uint_as_float(v[k]) : 0.0f;
+            }
           }
         }
       }
+    }
+    named_sync(1, kFbConvThreads);
+    if (!bad) {
+      float4 *o4 = reinterpret_cast<float4 *>(obox);
+      const float4 *s4 = reinterpret_cast<const float4 *>(sbox);
+      for (int i = threadIdx.x; i < nsh * box_floats / 4; i += kFbConvThreads) {
+        float4 a = o4[i];
+        const float4 b = s4[i];
+        a.x += b.x;
+        a.y += b.y;
+        a.z += b.z;
+        a.w += b.w;
+        o4[i] = a;
+      }
+      fence_proxy_async_smem();  // the box is read by the async proxy (TMA store)
+    }
+    named_sync(1, kFbConvThreads);
+    if (!bad && warp == 0) {
+      if (lane == 0) {
+        for (int sh = 0; sh < nsh; ++sh)
+          tma_store_4d(&omap, obox + (size_t)sh * box_floats, lblk * kFbLB, sp, cblk * p.CB * p.OH, s0 + sh);
+        bulk_commit_group();
+        bulk_wait_group_read0();  // the shared memory stays valid until read
+      }
+      __syncwarp();
     }
   } else if (warp == kFbMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
@@ -552,17 +582,18 @@ __global__ void __launch_bounds__(kFbThreads, 1)
       int u = 0;
       for (int q = q0; q < q1; ++u) {
         const FbStage st = fb_stage(p, q, q1);
-        const int slot = u & 1;
-        if (*abort || (u >= 2 && !mbar_wait(&fp_empty[slot], ((uint32_t)(u >> 1) & 1) ^ 1, p.err))) {
+        const int sslot = u % kFbStg;
+        if (*abort ||
+            (u >= kFbStg && !mbar_wait(&fp_empty[sslot], ((uint32_t)(u / kFbStg) & 1) ^ 1, p.err))) {
           *abort = 1;
           break;
         }
-        uint8_t *gdst = smem + (size_t)slot * p.stg_bytes;
+        uint8_t *gdst = smem + (size_t)sslot * p.stg_bytes;
         const int j0 = st.jb * 16;
-        mbar_arrive_expect_tx(&fp_full[slot], kFbGBytes + p.xbox_bytes);
-        tma_load_3d(gdst, &gmap, &fp_full[slot], CONV ? p.Wg - 16 - j0 : j0, CONV ? p.Hg - st.i - kFbGRows : st.i,
+        mbar_arrive_expect_tx(&fp_full[sslot], kFbGBytes + p.xbox_bytes);
+        tma_load_3d(gdst, &gmap, &fp_full[sslot], CONV ? p.Wg - 16 - j0 : j0, CONV ? p.Hg - st.i - kFbGRows : st.i,
                     st.b * p.L + lblk * kFbLB);
-        tma_load_3d(gdst + kFbGBytes, &xmap, &fp_full[slot], j0 + (s0 & ~3), st.i, st.b * p.C + cblk * p.CB);
+        tma_load_3d(gdst + kFbGBytes, &xmap, &fp_full[sslot], j0 + (s0 & ~3), st.i, st.b * p.C + cblk * p.CB);
         q += st.n;
       }
     }
@@ -589,9 +620,9 @@ __global__ void __launch_bounds__(256) fa_bank_reduce(const __grid_constant__ Fa
     const int qb = bi % ((quads + 15) / 16), scr = bi / ((quads + 15) / 16);  // scr = (s * C + c) * OH + r
     const int r = scr % p.OH, sc = scr / p.OH;
     const int cg = sc % p.C, s = sc / p.C;
-    const int nsplit = (s / 2 * 2 + 1 < p.OW ? 2 : 1) * p.S1;
+    const int nsplit = s / 2 < p.npairs ? p.P : p.Q;
     const int quad = qb * 16 + lq4;
-    const float4 *q = reinterpret_cast<const float4 *>(p.part + (size_t)scr * 2 * p.S1 * Lpad) + quad;
+    const float4 *q = reinterpret_cast<const float4 *>(p.part + (size_t)scr * p.NS * Lpad) + quad;
     float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (quad < quads) {
       for (int base = k; base < nsplit; base += 16 * 8) {
@@ -657,9 +688,9 @@ bool make_bank_params(const ConvGeom &g, int sms, FaBankParams *out) {
     const uint32_t kgb = (uint32_t)rows_max * cb * 16;  // one k group of a term's row tiles
     const uint32_t term = 2 * kgb;
     const uint32_t bop = 4 * term;                      // two result columns x (hi, lo)
-    const size_t smem = 2 * (size_t)stg + 2 * (size_t)bop;
-    // the epilogue's exchange (two columns x N x 64 lanes) reuses the staging and operands
-    if (smem > budget || (size_t)2 * cb * p.OH * 64 * 4 > smem) continue;
+    const size_t smem = kFbStg * (size_t)stg + 2 * (size_t)bop;
+    // the epilogue's boxes (two copies of two columns x N x 64 planes) reuse the staging and operands
+    if (smem > budget || (size_t)4 * cb * p.OH * 64 * 4 > smem) continue;
     const int nb = (p.C + cb - 1) / cb;
     if (found && nb >= best_blocks) continue;
     found = true;
@@ -683,9 +714,24 @@ bool make_bank_params(const ConvGeom &g, int sms, FaBankParams *out) {
   const long long nch = (long long)p.B * p.JB * p.Hg;
   if (nch < 1 || nch > 0x3fffffffLL) return false;
   p.nch = (int)nch;
-  const long long per_col = (long long)p.cblocks * p.lblocks * p.OW;
-  p.S1 = (int)std::max(1LL, std::min<long long>(sms / per_col, (p.nch + 1) / 2));
-  if (per_col * p.S1 > 0x7fffffffLL || (long long)p.OW * p.C * p.OH * p.lblocks * kFbLB * 2 * p.S1 > 0x7fffffffLL)
+  // Splits: one wave of CTAs.  A lone column's CTA converts and stages as
+  // much per chunk as a pair's for about 0.8 of its time (measured: 455
+  // against 574 cycles a chunk), so it gets 0.8 as many splits and every
+  // CTA has about the same work.
+  const long long cl = (long long)p.cblocks * p.lblocks;
+  p.npairs = p.OW / 2;
+  const bool lone = (p.OW & 1) != 0;
+  const long long per_cl = std::max(1LL, sms / cl);
+  if (p.npairs == 0) {
+    p.P = 1;
+    p.Q = (int)std::min<long long>(per_cl, p.nch);
+  } else {
+    p.P = (int)std::max(1LL, std::min<long long>((long long)(per_cl / (p.npairs + (lone ? 0.8 : 0.0))), p.nch));
+    p.Q = lone ? std::max(1, (int)(0.8 * p.P + 0.5)) : 0;
+  }
+  p.NS = std::max(p.P, p.Q);
+  if (cl * (p.npairs * p.P + p.Q) > 0x7fffffffLL ||
+      (long long)p.OW * p.C * p.OH * p.lblocks * kFbLB * p.NS > 0x7fffffffLL)
     return false;
   // more than 160 KB keeps one CTA per SM: its 512 tensor-memory columns are free
   p.smem = std::max(p.smem, (size_t)160 * 1024);
@@ -694,7 +740,7 @@ bool make_bank_params(const ConvGeom &g, int sms, FaBankParams *out) {
 }
 
 size_t bank_workspace_bytes(const FaBankParams &p) {
-  return (size_t)2 * p.S1 * p.OW * p.C * p.OH * p.lblocks * kFbLB * sizeof(float);
+  return (size_t)p.NS * p.OW * p.C * p.OH * p.lblocks * kFbLB * sizeof(float);
 }
 
 FaTcParams make_params(const ConvGeom &g, int sms) {
@@ -752,12 +798,21 @@ int launch_fa_bank(FaBankParams p, bool conv, const float *x, const float *f, fl
   rc = encode_tensor_map_3d_box(&xmap, x, (uint64_t)p.W, (uint64_t)p.H, (uint64_t)p.B * p.C, kFbXCols,
                                 (uint32_t)p.xrows, (uint32_t)p.CB);
   if (rc) return rc;
+  // partial sums [OW][C*OH][NS][Lpad]: a CTA stores [1][CB*OH][1][64] boxes
+  CUtensorMap omap;
+  const uint64_t Lpad = (uint64_t)p.lblocks * kFbLB;
+  const uint64_t odims[4] = {Lpad, (uint64_t)p.NS, (uint64_t)p.C * p.OH, (uint64_t)p.OW};
+  const uint64_t ostr[3] = {Lpad * 4, Lpad * p.NS * 4, Lpad * p.NS * p.C * p.OH * 4};
+  const uint32_t obox[4] = {(uint32_t)kFbLB, 1, (uint32_t)(p.CB * p.OH), 1};
+  rc = encode_tensor_map_f32(&omap, p.part, 4, odims, ostr, obox);
+  if (rc) return rc;
   auto kern = conv ? fa_bank_kernel<true> : fa_bank_kernel<false>;
   rc = check_cuda(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem),
                   "cudaFuncSetAttribute(fa_bank)");
   if (rc) return rc;
-  const long long grid = (long long)p.cblocks * p.lblocks * p.OW * p.S1;
-  rc = launch_pdl(kern, dim3((unsigned)grid), dim3(kFbThreads), p.smem, st, "fa_bank_kernel launch", p, gmap, xmap);
+  const long long grid = (long long)p.cblocks * p.lblocks * (p.npairs * p.P + p.Q);
+  rc = launch_pdl(kern, dim3((unsigned)grid), dim3(kFbThreads), p.smem, st, "fa_bank_kernel launch", p, gmap, xmap,
+                  omap);
   if (rc) return rc;
   const long long nblk = (long long)p.OW * p.C * p.OH * p.lblocks;  // < 2^31: the plan checks it
   const int blocks = (int)std::min<long long>(nblk, 148LL * 16);

@@ -121,12 +121,31 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// 4-D tiled TMA store from shared memory (x innermost, coordinates >= 0; the
+// box is clipped at the tensor's bounds), in the thread's bulk group.
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, const void *src, int x, int y, int z, int w) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];\n" ::"l"(
+          reinterpret_cast<uint64_t>(map)),
+      "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z), "r"(w)
+      : "memory");
+}
+__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// Waits until the thread's bulk stores have read their shared-memory source.
+__device__ __forceinline__ void bulk_wait_group_read0() {
+  asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
+}
+
 // Host: encode a 3-D fp32 tensor map (cols, rows, planes) with the given box;
 // out-of-bounds elements read as zero.  Returns CCT_OK or an error status.
 int encode_tensor_map_3d(CUtensorMap *map, const float *base, uint64_t cols, uint64_t rows,
                          uint64_t planes, uint32_t box_c, uint32_t box_r);
 int encode_tensor_map_3d_box(CUtensorMap *map, const float *base, uint64_t cols, uint64_t rows,
                              uint64_t planes, uint32_t box_c, uint32_t box_r, uint32_t box_z);
+// Host: an fp32 tensor map of `rank` (<= 5) dimensions, innermost first:
+// extents, byte strides of dimensions 1.. (multiples of 16), box extents.
+int encode_tensor_map_f32(CUtensorMap *map, const float *base, int rank, const uint64_t *dims,
+                          const uint64_t *strides, const uint32_t *box);
 
 }  // namespace cct
 

@@ -266,8 +266,10 @@ __global__ void fa_tc_reduce(const __grid_constant__ FaTcParams p, float *__rest
 // stored; gradient columns outside 0..Wg-1 come from TMA's zero fill.
 //
 // Warps 0-15 convert (fp32 staging -> A in tensor memory, B in shared
-// memory), warp 16 issues the MMAs, warp 17 issues the TMA loads of the fp32
-// staging: a gradient box [20 columns][7 rows][64 planes] and an image box
+// memory), warps 16 and 17 issue the MMAs of the first and second result
+// column (one issuing thread could not keep the tensor core fed: ~110
+// cycles an MMA against its 80 of work), warp 18 issues the TMA loads of the
+// fp32 staging: a gradient box [20 columns][7 rows][64 planes] and an image box
 // [20 columns][xrows][CB planes], three stages deep (a box took ~3k cycles
 // to land).  Their plane pitches are odd numbers of
 // 16-byte units, so the converters' float4 reads are conflict-free.  B
@@ -277,9 +279,9 @@ __global__ void fa_tc_reduce(const __grid_constant__ FaTcParams p, float *__rest
 // partial sums; fa_bank_reduce adds them in a fixed order.
 constexpr int kFbConvWarps = 16;
 constexpr int kFbConvThreads = 32 * kFbConvWarps;
-constexpr int kFbMmaWarp = 16;
-constexpr int kFbLoadWarp = 17;
-constexpr int kFbThreads = 32 * 18;
+constexpr int kFbMmaWarp = 16;                  // and 17: one issuing thread per result column
+constexpr int kFbLoadWarp = 18;
+constexpr int kFbThreads = 32 * 19;
 constexpr int kFbChunks = 5;                    // chunks per stage
 constexpr int kFbStg = 3;                       // fp32 staging slots: a load has two stages to land
 constexpr int kFbGCols = 20, kFbGRows = 5;      // gradient box (odd plane pitch in 16-byte units)
@@ -382,9 +384,9 @@ __global__ void __launch_bounds__(kFbThreads, 1)
     }
     for (int k = 0; k < 2; ++k) {
       mbar_init(&op_full[k], kFbConvWarps);
-      mbar_init(&op_empty[k], 1);             // MMA commit
+      mbar_init(&op_empty[k], 2);             // both issuers' commits
     }
-    mbar_init(&done, 1);
+    mbar_init(&done, 2);
     abort_flag = 0;
     fence_barrier_init();
   }
@@ -535,8 +537,11 @@ __global__ void __launch_bounds__(kFbThreads, 1)
       }
       __syncwarp();
     }
-  } else if (warp == kFbMmaWarp) {
-    // ------------------------------------------------------------ MMA issuer
+  } else if (warp == kFbMmaWarp || warp == kFbMmaWarp + 1) {
+    // ------------------------------------------------------------ MMA issuers
+    // warp 16: result column s0 (accumulator at column 0), warp 17: s0 + 1
+    // (at column N), if the CTA has it; both commit every stage
+    const int sh = warp - kFbMmaWarp;
     if (lane == 0) {
       const uint32_t idesc = idesc_bf16_f32(128, p.N);
       const uint64_t bt = smem_desc_kmajor(0, p.kg_bytes, 128);
@@ -545,8 +550,8 @@ __global__ void __launch_bounds__(kFbThreads, 1)
       // keeps running 32-bit descriptor words and no per-MMA branching.
       const uint32_t ops16 = smem_u32(ops) >> 4;
       const uint32_t cb16 = (uint32_t)p.CB, term16 = p.term_bytes >> 4;  // a row tile: CB rows of 16 bytes
-      const uint32_t d0 = tmem, d1 = tmem + (uint32_t)p.N;
-      const bool two = nsh == 2;
+      const uint32_t d = tmem + (uint32_t)(sh * p.N);
+      const bool mine = sh < nsh;
       uint32_t acc = 0;
       int u = 0;
       for (int q = q0; q < q1; ++u) {
@@ -557,16 +562,14 @@ __global__ void __launch_bounds__(kFbThreads, 1)
           break;
         }
         tc_fence_after();
-        uint32_t a1 = tmem + kFbAcol + (uint32_t)(slot * kFbChunks) * 16;
-        uint32_t bw = b_lo + ops16 + ((uint32_t)slot * p.bop_bytes >> 4);
-        for (int k = 0; k < st.n; ++k, a1 += 16, bw += cb16) {
-          mma_bf16_ts(d0, a1, desc_word(b_hi, bw), idesc, acc);
-          mma_bf16_ts(d0, a1 + 8, desc_word(b_hi, bw + term16), idesc, 1u);
-          if (two) {
-            mma_bf16_ts(d1, a1, desc_word(b_hi, bw + 2 * term16), idesc, acc);
-            mma_bf16_ts(d1, a1 + 8, desc_word(b_hi, bw + 3 * term16), idesc, 1u);
+        if (mine) {
+          uint32_t a1 = tmem + kFbAcol + (uint32_t)(slot * kFbChunks) * 16;
+          uint32_t bw = b_lo + ops16 + ((uint32_t)slot * p.bop_bytes >> 4) + 2u * sh * term16;
+          for (int k = 0; k < st.n; ++k, a1 += 16, bw += cb16) {
+            mma_bf16_ts(d, a1, desc_word(b_hi, bw), idesc, acc);
+            mma_bf16_ts(d, a1 + 8, desc_word(b_hi, bw + term16), idesc, 1u);
+            acc = 1u;
           }
-          acc = 1u;
         }
         tc_commit(&op_empty[slot]);  // frees the stage once its MMAs are done
         q += st.n;
@@ -606,56 +609,55 @@ __global__ void __launch_bounds__(kFbThreads, 1)
 }
 
 // out[l*C + c](r, s) = the CTAs' partial sums for (s, c, r, l) in a fixed
-// order.  A block serves one (s, c, r), whose partial sums are one
-// contiguous run [split][planes]: thread (quad, k) loads four planes of every
-// sixteenth split from k (all its loads in flight at once), and the sixteen
-// sums of each plane are added in a fixed tree.
-__global__ void __launch_bounds__(256) fa_bank_reduce(const __grid_constant__ FaBankParams p, float *__restrict__ y) {
-  __shared__ float4 red[16][17];
+// order.  A block of 128 threads serves one (s, c, r) and 64 planes, whose
+// partial sums are one contiguous run [split][planes]: thread (k, quad) adds
+// four planes of the splits k, k + 8, ... in split order (eight loads in
+// flight), and one thread per quad adds the eight sums in lane order.
+__global__ void __launch_bounds__(128) fa_bank_reduce(const __grid_constant__ FaBankParams p, float *__restrict__ y) {
+  __shared__ float4 red[8][16];
   grid_dependency_wait();
   const int Lpad = p.lblocks * kFbLB, quads = Lpad / 4;
-  const int k = threadIdx.x >> 4, lq4 = threadIdx.x & 15;
-  const int nblk = p.OW * p.C * p.OH * ((quads + 15) / 16);
+  const int quad16 = threadIdx.x & 15, k = threadIdx.x >> 4;
+  const int nblk = p.OW * p.C * p.OH * p.lblocks;
   for (int bi = blockIdx.x; bi < nblk; bi += gridDim.x) {
-    const int qb = bi % ((quads + 15) / 16), scr = bi / ((quads + 15) / 16);  // scr = (s * C + c) * OH + r
-    const int r = scr % p.OH, sc = scr / p.OH;
-    const int cg = sc % p.C, s = sc / p.C;
+    const int lb = bi % p.lblocks, scr = bi / p.lblocks;  // scr = (s * C + c) * OH + r
+    const int s = scr / (p.C * p.OH);
     const int nsplit = s / 2 < p.npairs ? p.P : p.Q;
-    const int quad = qb * 16 + lq4;
-    const float4 *q = reinterpret_cast<const float4 *>(p.part + (size_t)scr * p.NS * Lpad) + quad;
+    const float4 *q = reinterpret_cast<const float4 *>(p.part + (size_t)scr * p.NS * Lpad) + lb * 16 + quad16;
     float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (quad < quads) {
-      for (int base = k; base < nsplit; base += 16 * 8) {
-        float4 v[8];
+    for (int base = k; base < nsplit; base += 64) {
+      float4 v[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          v[j] = base + 16 * j < nsplit ? q[(size_t)(base + 16 * j) * quads] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      for (int j = 0; j < 8; ++j)
+        v[j] = base + 8 * j < nsplit ? q[(size_t)(base + 8 * j) * quads] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          acc.x += v[j].x;
-          acc.y += v[j].y;
-          acc.z += v[j].z;
-          acc.w += v[j].w;
-        }
+      for (int j = 0; j < 8; ++j) {
+        acc.x += v[j].x;
+        acc.y += v[j].y;
+        acc.z += v[j].z;
+        acc.w += v[j].w;
       }
     }
-    red[k][lq4] = acc;
+    red[k][quad16] = acc;
     __syncthreads();
-    if (threadIdx.x < 64) {
-      // plane 4 * (qb * 16 + t / 4) + t % 4: the sixteen split lanes in a fixed tree
-      const int t = threadIdx.x, qq = t >> 2, comp = t & 3;
-      float w[16];
+    if (threadIdx.x < 16) {
+      float4 t = red[0][threadIdx.x];
 #pragma unroll
-      for (int kk = 0; kk < 16; ++kk) {
-        const float4 a = red[kk][qq];
-        w[kk] = comp == 0 ? a.x : comp == 1 ? a.y : comp == 2 ? a.z : a.w;
+      for (int kk = 1; kk < 8; ++kk) {
+        const float4 u = red[kk][threadIdx.x];
+        t.x += u.x;
+        t.y += u.y;
+        t.z += u.z;
+        t.w += u.w;
       }
-#pragma unroll
-      for (int h = 8; h >= 1; h >>= 1)
-#pragma unroll
-        for (int kk = 0; kk < h; ++kk) w[kk] += w[kk + h];
-      const int l = 4 * (qb * 16 + qq) + comp;
-      if (l < p.L) y[((size_t)l * p.C + cg) * p.OH * p.OW + (size_t)r * p.OW + s] = w[0];
+      const int cr = scr - s * p.C * p.OH, c = cr / p.OH, r = cr - c * p.OH;
+      const int l0 = lb * kFbLB + 4 * threadIdx.x;
+      const size_t plane = (size_t)p.C * p.OH * p.OW;
+      float *o = y + ((size_t)l0 * p.C + c) * p.OH * p.OW + (size_t)r * p.OW + s;
+      if (l0 < p.L) o[0] = t.x;
+      if (l0 + 1 < p.L) o[plane] = t.y;
+      if (l0 + 2 < p.L) o[2 * plane] = t.z;
+      if (l0 + 3 < p.L) o[3 * plane] = t.w;
     }
     __syncthreads();
   }
@@ -816,7 +818,7 @@ int launch_fa_bank(FaBankParams p, bool conv, const float *x, const float *f, fl
   if (rc) return rc;
   const long long nblk = (long long)p.OW * p.C * p.OH * p.lblocks;  // < 2^31: the plan checks it
   const int blocks = (int)std::min<long long>(nblk, 148LL * 16);
-  rc = launch_pdl(fa_bank_reduce, dim3(blocks), dim3(256), 0, st, "fa_bank_reduce launch", p, y);
+  rc = launch_pdl(fa_bank_reduce, dim3(blocks), dim3(128), 0, st, "fa_bank_reduce launch", p, y);
   if (rc) return rc;
   count_launches(2);
   return CCT_OK;

@@ -1,9 +1,13 @@
 // FilterAdjointBlockReduceSum (the weight gradient) on the tcgen05 tensor
 // cores in split-BF16 precision, for the shapes fa_f32 serves (BorderValid,
-// no sampling, small results):
+// no sampling):
 //   out[l*C + c](r, s) = sum_b sum_(i,j) x[b*C + c](r + i, s + j) * g'[b*L + l](i, j)
 // (ConvolveHyperKernel.scala:187, 333, 575-590; CogFunctionAPI.scala:1480-1511;
-// g' = g flipped for convolveFilterAdjoint).
+// g' = g flipped for convolveFilterAdjoint).  Two forms:
+// - the gradient-planes form (fa_bank_kernel, below): gradient planes as the
+//   MMA rows, (result row, image plane) as the columns, one accumulator per
+//   result column; taken when the rows suit TMA and OH * CB <= 160;
+// - the im2col form (fa_tc_kernel) for the other shapes:
 //
 // GEMM view: D[m][n] = sum_k A[m][k] B[n][k] with rows m = (c, r, s) of the
 // result (M = C*OH*OW), columns n = l (the gradient planes) and the reduction
@@ -269,10 +273,10 @@ __global__ void fa_tc_reduce(const __grid_constant__ FaTcParams p, float *__rest
 // memory), warps 16 and 17 issue the MMAs of the first and second result
 // column (one issuing thread could not keep the tensor core fed: ~110
 // cycles an MMA against its 80 of work), warp 18 issues the TMA loads of the
-// fp32 staging: a gradient box [20 columns][7 rows][64 planes] and an image box
+// fp32 staging: a gradient box [20 columns][5 rows][64 planes] and an image box
 // [20 columns][xrows][CB planes], three stages deep (a box took ~3k cycles
-// to land).  Their plane pitches are odd numbers of
-// 16-byte units, so the converters' float4 reads are conflict-free.  B
+// to land).  Their plane pitches are odd numbers of 16-byte units, so the
+// converters' float4 reads are conflict-free.  B
 // layout: [k group][row tile][8-row group][8 rows][16 B], 8-row groups
 // adjacent, which the tensor core reads at its full rate.  Each CTA reduces
 // a contiguous range of chunks, adds its two row halves and stores its

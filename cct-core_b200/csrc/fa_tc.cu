@@ -537,7 +537,10 @@ __global__ void __launch_bounds__(kFbThreads, 1)
         for (int sh = 0; sh < nsh; ++sh)
           tma_store_4d(&omap, obox + (size_t)sh * box_floats, lblk * kFbLB, sp, cblk * p.CB * p.OH, s0 + sh);
         bulk_commit_group();
-        bulk_wait_group_read0();  // the shared memory stays valid until read
+        // the shared memory must stay valid until the stores have read it;
+        // their global writes are part of this grid's completion, which the
+        // reduce kernel's grid_dependency_wait() (and stream order) waits for
+        bulk_wait_group_read0();
       }
       __syncwarp();
     }

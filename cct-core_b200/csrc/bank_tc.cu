@@ -189,12 +189,15 @@ __device__ __forceinline__ ItemUnits item_units(const BankParams &p, const Item 
 // the first plane; `cvalid` planes exist (the rest are zero).  All 8*KG loads
 // are issued before the first store, so a converter thread keeps that many
 // reads in flight.
-template <int TERMS, int KG>
-__device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, bool in, int cvalid,
-                                                uint8_t *dst, uint32_t kg_stride, uint32_t part_bytes) {
-  float v[8 * KG];
+template <int KG>
+__device__ __forceinline__ void load_kgroups(const float *src, size_t plane, bool in, int cvalid, float (&v)[8 * KG]) {
 #pragma unroll
   for (int j = 0; j < 8 * KG; ++j) v[j] = (in && j < cvalid) ? __ldg(src + j * plane) : 0.0f;
+}
+
+template <int TERMS, int KG>
+__device__ __forceinline__ void store_kgroups(const float (&v)[8 * KG], uint8_t *dst, uint32_t kg_stride,
+                                              uint32_t part_bytes) {
 #pragma unroll
   for (int k = 0; k < KG; ++k) {
     uint8_t *d = dst + k * kg_stride;
@@ -214,6 +217,14 @@ __device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, 
       *reinterpret_cast<uint4 *>(d + 2 * (size_t)part_bytes) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
     }
   }
+}
+
+template <int TERMS, int KG>
+__device__ __forceinline__ void convert_kgroups(const float *src, size_t plane, bool in, int cvalid,
+                                                uint8_t *dst, uint32_t kg_stride, uint32_t part_bytes) {
+  float v[8 * KG];
+  load_kgroups<KG>(src, plane, in, cvalid, v);
+  store_kgroups<TERMS, KG>(v, dst, kg_stride, part_bytes);
 }
 
 // Final accumulator of work item `it` (S in tensor-memory columns at `sc`,
@@ -351,7 +362,9 @@ __device__ __forceinline__ void store_tile_columns(const BankParams &p, const It
 // accumulator phase in order) and a quarter of a tile is whole chunks.
 __device__ __forceinline__ bool helpers_store_last(const BankParams &p) { return !p.promote && p.N % 64 == 0; }
 
-template <int TERMS, bool PAIR>
+// CB16: 16-plane blocks (the converters pair their (phase, position) items);
+// a separate instance, so the other plane blocks' code is unchanged.
+template <int TERMS, bool PAIR, bool CB16>
 __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_constant__ BankParams p) {
   extern __shared__ __align__(1024) uint8_t smem[];
   __shared__ Bars bars;
@@ -418,24 +431,54 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
         uint8_t *hbase = halo + (size_t)buf * p.halo_bytes;
         const int cv = g.n - cb * p.CB;  // planes of this block that exist
         const float *xc = xb + (size_t)cb * p.CB * plane;
-        for (int ph = 0; ph < p.nphase; ++ph) {
-          uint8_t *hph = hbase + (size_t)ph * TERMS * p.part_bytes;
-          for (int q = threadIdx.x; q < p.L; q += kConvThreads) {
-            const int G = p0 + q;
-            const int Y = G / p.P, X = G - Y * p.P;
-            const int iy = g.down * (Y + row0) + p.phase_r[ph];
-            const int ix = g.down * (col0 + X) + p.phase_c[ph];
-            int ry, rx;
-            const bool in = border_map(g, iy, ix, ry, rx);
-            const float *src = in ? xc + (size_t)ry * g.W + rx : xc;
-            uint8_t *dst = hph + (size_t)q * 16;
-            int kg = 0;
-            for (; kg + 4 <= nkg; kg += 4)
-              convert_kgroups<TERMS, 4>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
-                                        kgs, p.part_bytes);
-            for (; kg < nkg; kg += 2)
-              convert_kgroups<TERMS, 2>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
-                                        kgs, p.part_bytes);
+        if constexpr (CB16) {
+          // 16-plane blocks: the (phase, position) items two at a time, both
+          // items' loads issued before either is converted, so a thread has
+          // as many loads in flight as with a 32-plane position
+          const int total = p.nphase * p.L;
+          for (int it = threadIdx.x; it < total; it += 2 * kConvThreads) {
+            const float *src[2];
+            bool in[2];
+            uint8_t *dst[2];
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const int item = min(it + e * kConvThreads, total - 1);
+              const int ph = item / p.L, q = item - ph * p.L;
+              const int G = p0 + q;
+              const int Y = G / p.P, X = G - Y * p.P;
+              const int iy = g.down * (Y + row0) + p.phase_r[ph];
+              const int ix = g.down * (col0 + X) + p.phase_c[ph];
+              int ry, rx;
+              in[e] = border_map(g, iy, ix, ry, rx);
+              src[e] = in[e] ? xc + (size_t)ry * g.W + rx : xc;
+              dst[e] = hbase + (size_t)ph * TERMS * p.part_bytes + (size_t)q * 16;
+            }
+            float va[16], vb[16];
+            load_kgroups<2>(src[0], plane, in[0], cv, va);
+            load_kgroups<2>(src[1], plane, in[1], cv, vb);
+            store_kgroups<TERMS, 2>(va, dst[0], kgs, p.part_bytes);
+            if (it + kConvThreads < total) store_kgroups<TERMS, 2>(vb, dst[1], kgs, p.part_bytes);
+          }
+        } else {
+          for (int ph = 0; ph < p.nphase; ++ph) {
+            uint8_t *hph = hbase + (size_t)ph * TERMS * p.part_bytes;
+            for (int q = threadIdx.x; q < p.L; q += kConvThreads) {
+              const int G = p0 + q;
+              const int Y = G / p.P, X = G - Y * p.P;
+              const int iy = g.down * (Y + row0) + p.phase_r[ph];
+              const int ix = g.down * (col0 + X) + p.phase_c[ph];
+              int ry, rx;
+              const bool in = border_map(g, iy, ix, ry, rx);
+              const float *src = in ? xc + (size_t)ry * g.W + rx : xc;
+              uint8_t *dst = hph + (size_t)q * 16;
+              int kg = 0;
+              for (; kg + 4 <= nkg; kg += 4)
+                convert_kgroups<TERMS, 4>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
+                                          kgs, p.part_bytes);
+              for (; kg < nkg; kg += 2)
+                convert_kgroups<TERMS, 2>(src + (size_t)kg * 8 * plane, plane, in, cv - kg * 8, dst + (size_t)kg * kgs,
+                                          kgs, p.part_bytes);
+            }
           }
         }
         // the tensor core reads the halo through the async proxy
@@ -806,15 +849,15 @@ __global__ void __launch_bounds__(kPackThreads, 16) bank_pack_kernel(const __gri
 std::mutex g_bank_mu;
 std::unordered_map<uint64_t, size_t> g_bank_attr;
 
-template <int TERMS, bool PAIR>
+template <int TERMS, bool PAIR, bool CB16>
 int launch_terms(const BankParams &p, cudaStream_t st) {
-  auto kern = bank_tc_kernel<TERMS, PAIR>;
+  auto kern = bank_tc_kernel<TERMS, PAIR, CB16>;
   {
     // Dynamic shared memory above 48 KB needs the opt-in attribute; keep the
     // largest size set so far per (device, instance).
     int dev = 0;
     cudaGetDevice(&dev);
-    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)(TERMS * 2 + (PAIR ? 1 : 0));
+    const uint64_t key = ((uint64_t)dev << 32) | (uint64_t)(TERMS * 4 + (PAIR ? 2 : 0) + (CB16 ? 1 : 0));
     std::lock_guard<std::mutex> lk(g_bank_mu);
     size_t &have = g_bank_attr[key];
     if (have < p.smem_bytes) {
@@ -1064,8 +1107,10 @@ int launch_bank_tc(const BankParams &p, const float *x, float *y, const uint8_t 
   if ((reinterpret_cast<uintptr_t>(y) & 15) != 0) q.vec4 = 0;  // float4 stores need a 16-byte aligned output
   q.bpack = packed;
   q.err = err;
-  if (p.pair) return launch_terms<2, true>(q, st);
-  return p.terms == 2 ? launch_terms<2, false>(q, st) : launch_terms<3, false>(q, st);
+  const bool cb16 = p.CB == 16;
+  if (p.pair) return cb16 ? launch_terms<2, true, true>(q, st) : launch_terms<2, true, false>(q, st);
+  if (p.terms == 2) return cb16 ? launch_terms<2, false, true>(q, st) : launch_terms<2, false, false>(q, st);
+  return cb16 ? launch_terms<3, false, true>(q, st) : launch_terms<3, false, false>(q, st);
 }
 
 }  // namespace cct

@@ -36,20 +36,20 @@
 // afresh, which bounds the accumulation error by the segment length.  The
 // epilogue adds each filter's big and small rows.
 //
-// Warp roles (one persistent CTA per SM, 576 threads):
-//   warps 0-7   converters: for each (tile, plane block) fill a halo buffer:
+// Warp roles (one persistent CTA per SM, 640 threads):
+//   warps 0-9   converters: for each (tile, plane block) fill a halo buffer:
 //               plain loads of the input with the border policy applied
 //               (zero, clamp, cyclic), split into bf16 terms, stored in the
 //               K-major core-matrix layout [plane group][position][8 planes];
 //               two buffers, so the next block is converted while the
-//               current one is multiplied.  Then they store half of the
-//               CTA's last tile with the epilogue warps.
-//   warp 8      MMA issuer (one elected lane): per (tile, plane block, tap):
+//               current one is multiplied.  Then warps 0-7 store half of
+//               the CTA's last tile with the epilogue warps.
+//   warp 10     MMA issuer (one elected lane): per (tile, plane block, tap):
 //               KS k-steps x nmma MMAs, A = filter chunk stage, B = halo.
-//   warp 9      loader (one lane): bulk copies of the pre-packed filter
+//   warp 11     loader (one lane): bulk copies of the pre-packed filter
 //               chunks (nb, plane block, tap) into a ring of stages, one copy
 //               per stage of several taps.
-//   warps 10-17 epilogue, two per tensor-memory lane quarter (alternate
+//   warps 12-19 epilogue, two per tensor-memory lane quarter (alternate
 //               column halves): promotion adds, then per 16-column chunk the
 //               warps holding one filter block's parts write them to shared
 //               memory, and each adds the parts of a share of the filters,
@@ -69,7 +69,7 @@
 namespace cct {
 namespace {
 
-constexpr int kConvWarps = 8;
+constexpr int kConvWarps = 10;  // ten: a 536-position halo takes two rounds of loads, not three
 constexpr int kConvThreads = 32 * kConvWarps;
 constexpr int kMmaWarp = kConvWarps;
 constexpr int kLoadWarp = kConvWarps + 1;
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 1) bank_tc_kernel(const __grid_const
       }
     }
     if (failed) *abort_flag = 1;
-    if (helpers_store_last(p) && blockIdx.x < p.total) {
+    if (helpers_store_last(p) && blockIdx.x < p.total && warp < 8) {
       // The CTA's last tile, upper half of the columns: wait for its
       // accumulator (one segment per item, so the phases of each buffer are
       // waited in order), then store through tiles in the halo, which no MMA
